@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Throughput of the Huffman-with-gap-arrays path on B200.
+
+One step = one full pass of the path over the workload buffer:
+histogram (GPU) -> codebook (host, from the 1 KiB histogram) -> fused encode
+(GPU) -> decode (GPU), i.e. the reference's bin/encoder followed by
+bin/decoder minus file I/O.  The default workload is the large single-buffer
+config: 1 GiB of 1 MiB blocks, each Zipf(1.05) or 8-bit quantised N(0,1),
+seeded (inputs > L2, so no flush is needed between steps).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    torchrun --nproc-per-node N bench.py --gpus N ...   (N > 1: one replica per GPU)
+
+Prints one JSON line.  `value` = uncompressed bytes of all ranks / (max over
+ranks of the device time of K steps); `e2e` = the same through the public API
+with pinned host buffers and the H2D/D2H copies inside the timed region.
+The path partitions by buffer, so N GPUs run N independent replicas (weak
+scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "enc/dec GB/s of raw bytes, % HBM roofline; batched+tuned vs plain on 1 B200"
+WORKLOADS = {
+    "mixed_1g": ("1 GiB uint8, 1 MiB blocks of Zipf(1.05) or 8-bit quantised N(0,1) "
+                 "(+-3 sigma -> 0..255), block kind by hash(seed, block), seed 2", 1 << 30),
+    "zipf_16m": ("16 MiB uint8 i.i.d. Zipf(s=1.2) over 256 symbols, seed 1", 16 << 20),
+    "mixed_256m": ("256 MiB prefix-sized version of the mixed workload (profiling case)", 256 << 20),
+}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="hgap", choices=["hgap", "reference"])
+    p.add_argument("--workload", default="mixed_1g", choices=sorted(WORKLOADS))
+    p.add_argument("--cpu-sample-mib", type=int, default=256)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_ratios():
+    """DRAM bytes per uncompressed byte per kernel, from the committed ncu summary."""
+    out = {}
+    path = os.path.join(ROOT, "profiles", "dram_traffic_mixed_1g.txt")
+    if not os.path.exists(path):
+        return out
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == "traffic_per_input_byte":
+            out[parts[1]] = float(parts[2])
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        import torch
+        self.proc = None
+        try:
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            ident = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+            self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", ident, "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[3:7]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.out.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_roundtrip(x_np, threads: int):
+    """The oracle (CPU restatement of the reference path) over one sample:
+    histogram -> codebook -> encode -> decode, all host threads."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    h = O.histogram_mt(x_np, threads)
+    cb = O.codebook(h)
+    bits, gaps = O.encode_mt(x_np, cb, cb.total_bits, threads)
+    y = O.decode_mt(bits, gaps, (cb.total_bits + 127) // 128, cb, x_np.size, threads)
+    dt = time.perf_counter() - t0
+    return dt, y
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def make_workload(name: str, device, rank: int = 0):
+    from huffman_coding_gap_arrays_b200 import workloads as WL
+    if name in ("mixed_1g", "mixed_256m"):
+        return WL.mixed_buffer(WORKLOADS[name][1], seed=2 + 1000 * rank, device=device)
+    return WL.zipf_buffer(16 << 20, 1.2, seed=1 + 1000 * rank, device=device)
+
+
+def run_reference(args, rank: int, world: int):
+    """`--impl reference`: the reference path's CPU implementation (the oracle
+    port -- the reference itself has no CPU encoder/decoder) on the box's host
+    cores, on a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+    desc, n_full = WORKLOADS[args.workload]
+    x = make_workload(args.workload, "cpu")
+    sample = min(n_full, args.cpu_sample_mib << 20)
+    xs = np.ascontiguousarray(x[:sample].numpy())
+    threads = host_threads()
+    for _ in range(args.warmup):
+        cpu_roundtrip(xs, threads)
+    times = []
+    for _ in range(args.steps):
+        dt, y = cpu_roundtrip(xs, threads)
+        times.append(dt)
+    assert np.array_equal(y, xs)
+    t = sum(times)
+    value = sample * args.steps / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * t / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": desc, "bytes": n_full, "sample_bytes": sample},
+        "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": f"first {sample >> 20} MiB of the workload, histogram+codebook+"
+                                   f"encode+decode per step (oracle/hgap_oracle.c, pthreads)"},
+        "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    del torch
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    import huffman_coding_gap_arrays_b200 as H
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+        pg = dist
+
+    desc, n = WORKLOADS[args.workload]
+    x = make_workload(args.workload, dev, rank)
+    stream = torch.cuda.current_stream()
+    hist = torch.empty(256, dtype=torch.int32, device=dev)
+    hist_host = torch.empty(256, dtype=torch.int32, pin_memory=True)
+
+    # size the outputs once from the histogram (worst case: 16 bits per byte is
+    # never needed; W for this buffer is fixed)
+    H.histogram(x, out=hist)
+    book0, sizes0 = H.Codebook.from_histogram(hist.cpu())
+    bits = torch.empty(sizes0.words + 16, dtype=torch.int32, device=dev)
+    gaps = torch.empty(sizes0.gap_words + 16, dtype=torch.int32, device=dev)
+    out = torch.empty(n + 16, dtype=torch.uint8, device=dev)
+    enc = H.Encoder(n, dev)
+    dec = H.Decoder(sizes0.segments, dev)
+
+    ev = {k: [] for k in ("hist", "encode", "decode")}
+
+    def step(record: bool):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(6)] if record else None
+        if record:
+            e[0].record(stream)
+        H.histogram(x, out=hist)
+        if record:
+            e[1].record(stream)
+        hist_host.copy_(hist, non_blocking=True)
+        stream.synchronize()
+        book, sizes = H.Codebook.from_histogram(hist_host)
+        if record:
+            e[2].record(stream)
+        enc.encode(x, book, sizes, bits=bits, gaps=gaps, check_status=False)
+        if record:
+            e[3].record(stream)
+            e[4].record(stream)
+        dec.decode(bits, gaps, sizes, book, n, out=out, check_status=False)
+        if record:
+            e[5].record(stream)
+            ev["hist"].append((e[0], e[1]))
+            ev["encode"].append((e[2], e[3]))
+            ev["decode"].append((e[4], e[5]))
+        return book, sizes
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    enc.check()
+    dec.check()
+    if not torch.equal(out[:n], x):
+        raise SystemExit("decode(encode(x)) != x")
+
+    clocks = ClockSampler(local) if rank == 0 else None
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        book, sizes = step(True)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clock_info = clocks.stop() if clocks else None
+    ms = t0.elapsed_time(t1)
+    enc.check()
+    dec.check()
+    if not torch.equal(out[:n], x):
+        raise SystemExit("decode(encode(x)) != x after the timed steps")
+    if pg:
+        tm = torch.tensor([ms], device=dev)
+        pg.all_reduce(tm, op=pg.ReduceOp.MAX)
+        ms = float(tm.item())
+
+    kern_ms = {k: sum(a.elapsed_time(b) for a, b in v) / len(v) for k, v in ev.items()}
+    C = 4 * (sizes.words + sizes.gap_words)
+    alg = {"hist": n, "encode": n + C, "decode": C + n}
+    peak, peak_src = peak_hbm()
+    kernels = {k: {"ms": round(kern_ms[k], 4),
+                   "raw_gbs": round(n / kern_ms[k] / 1e6, 1),
+                   "alg_gbs": round(alg[k] / kern_ms[k] / 1e6, 1),
+                   "frac_of_" + peak_src: round(alg[k] / kern_ms[k] / 1e6 / peak, 4)}
+               for k in kern_ms}
+    dom = max(kern_ms, key=kern_ms.get)
+    achieved = alg[dom] / kern_ms[dom] / 1e6
+    tr = traffic_ratios()
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": (round(tr[dom] * n) if dom in tr else None),
+                "algorithmic_bytes": alg[dom]}
+
+    # ---- end to end through the public API, host buffers -------------------
+    e2e = None
+    if not args.no_e2e:
+        x_host = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        x_host.copy_(x)
+        bits_host = torch.empty(sizes.words, dtype=torch.int32, pin_memory=True)
+        gaps_host = torch.empty(sizes.gap_words, dtype=torch.int32, pin_memory=True)
+        y_host = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        x_dev = torch.empty_like(x)
+        bits_in = torch.empty_like(bits)
+        gaps_in = torch.empty_like(gaps)
+
+        def e2e_step():
+            x_dev.copy_(x_host, non_blocking=True)                      # H2D input
+            H.histogram(x_dev, out=hist)
+            hist_host.copy_(hist, non_blocking=True)
+            stream.synchronize()
+            book, sz = H.Codebook.from_histogram(hist_host)
+            b, g = enc.encode(x_dev, book, sz, bits=bits, gaps=gaps, check_status=False)
+            bits_host[:sz.words].copy_(b, non_blocking=True)            # D2H container payload
+            gaps_host[:sz.gap_words].copy_(g, non_blocking=True)
+            bits_in[:sz.words].copy_(bits_host[:sz.words], non_blocking=True)   # H2D for decode
+            gaps_in[:sz.gap_words].copy_(gaps_host[:sz.gap_words], non_blocking=True)
+            dec.decode(bits_in, gaps_in, sz, book, n, out=out, check_status=False)
+            y_host.copy_(out[:n], non_blocking=True)                   # D2H output
+            return sz
+
+        e2e_steps = max(2, args.steps // 2)
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b_ = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(e2e_steps):
+            sz = e2e_step()
+        b_.record(stream)
+        torch.cuda.synchronize()
+        e_ms = a.elapsed_time(b_)
+        enc.check()
+        dec.check()
+        if not torch.equal(y_host, x_host):
+            raise SystemExit("e2e round trip mismatch")
+        if pg:
+            tm = torch.tensor([e_ms], device=dev)
+            pg.all_reduce(tm, op=pg.ReduceOp.MAX)
+            e_ms = float(tm.item())
+        cbytes = 4 * (sz.words + sz.gap_words)
+        e2e = {"value": round(world * n * e2e_steps / e_ms / 1e6, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": n + cbytes, "d2h_bytes_per_step": cbytes + n,
+               "ms_per_step": round(e_ms / e2e_steps, 3)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = host_threads()
+        sample = min(n, args.cpu_sample_mib << 20)
+        xs = np.ascontiguousarray(x[:sample].cpu().numpy())
+        cpu_roundtrip(xs, threads)
+        dt, y = cpu_roundtrip(xs, threads)
+        assert np.array_equal(y, xs)
+        cpu = {"value": round(sample / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": f"first {sample >> 20} MiB of the workload, one histogram+codebook+encode+"
+                         f"decode round trip (oracle/hgap_oracle.c, pthreads)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": round(world * n * args.steps / ms / 1e6, 3),
+            "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8", "data": "synthetic",
+            "config": {"workload": desc, "bytes_per_gpu": n, "parallelism": f"replicas x{world}",
+                       "step": "histogram -> codebook (host) -> encode -> decode",
+                       "l2": "input (1 GiB) larger than the 126 MB L2; no flush",
+                       "compressed_bytes": C, "bits_per_byte": round(sizes.bits / n, 4)},
+            "encode_gbs": round(n / (kern_ms["hist"] + kern_ms["encode"]) / 1e6, 1),
+            "decode_gbs": round(n / kern_ms["decode"] / 1e6, 1),
+            "kernels": kernels,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": 3 * args.steps,
+            "clocks": clock_info,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

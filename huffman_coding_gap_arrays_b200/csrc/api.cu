@@ -1,0 +1,133 @@
+// api.cu -- the extern "C" device entry points of libhgap.so (include/hgap.h).
+// Validation, workspace carving and launches; no allocation anywhere.
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "hgap_internal.h"
+
+namespace {
+
+using hgap::kWsHeader;
+
+inline bool aligned(const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; }
+
+inline hgap_status cuda_status(int e) { return e == 0 ? HGAP_OK : HGAP_ERR_CUDA; }
+
+// Recomputes the canonical codes from the book's own symbol list, so a
+// hand-edited table can never reach the decoder inconsistent.
+hgap_status canonical_copy(const hgap_codebook* in, hgap_codebook* out) {
+    if (in->symbol_count > 256) return HGAP_ERR_CORRUPT;
+    return hgap_codebook_from_symbols(in->symbols, in->symbol_count, out);
+}
+
+}  // namespace
+
+extern "C" {
+
+hgap_status hgap_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, hgap_stream_t stream) {
+    if (!d_hist || (n && !d_in)) return HGAP_ERR_INVALID_ARG;
+    return cuda_status(hgap::launch_histogram(d_in, n, d_hist, stream));
+}
+
+size_t hgap_encode_workspace_bytes(uint64_t n) {
+    return kWsHeader + 3 * sizeof(uint64_t) * (size_t)hgap::encode_tiles(n);
+}
+
+hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
+                        uint64_t words, uint32_t* d_gaps, uint64_t segments, void* d_workspace,
+                        size_t workspace_bytes, hgap_stream_t stream) {
+    if (!cb) return HGAP_ERR_INVALID_ARG;
+    if (n == 0) return (words == 0 && segments == 0) ? HGAP_OK : HGAP_ERR_SIZE;
+    if (!d_in || !d_bits || !d_gaps || !d_workspace) return HGAP_ERR_INVALID_ARG;
+    if (!aligned(d_bits, 4) || !aligned(d_gaps, 4) || !aligned(d_workspace, 8))
+        return HGAP_ERR_INVALID_ARG;
+    if (segments != (words + 3) / 4 || words == 0) return HGAP_ERR_SIZE;
+    for (int b = 0; b < 256; ++b) {
+        const uint32_t l = cb->table[b].length;
+        if (l > (uint32_t)hgap::kMaxLen || (l && (cb->table[b].code >> l) != 0)) return HGAP_ERR_CORRUPT;
+    }
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(d_in);
+    hgap::EncArgs a;
+    a.lo = addr & 15;
+    a.hi = a.lo + n;
+    a.in_aligned = reinterpret_cast<const uint8_t*>(addr - a.lo);
+    a.ntiles = (a.hi + hgap::kEncTileBytes - 1) / hgap::kEncTileBytes;
+    if (a.ntiles >= 0xffffffffull) return HGAP_ERR_UNSUPPORTED;
+    const size_t need = kWsHeader + 3 * sizeof(uint64_t) * (size_t)a.ntiles;
+    if (workspace_bytes < need) return HGAP_ERR_WORKSPACE;
+    uint8_t* ws = static_cast<uint8_t*>(d_workspace);
+    a.status = reinterpret_cast<uint32_t*>(ws);
+    a.counter = reinterpret_cast<uint32_t*>(ws) + 1;
+    a.lookback = reinterpret_cast<uint64_t*>(ws + kWsHeader);
+    a.hand_bits = a.lookback + a.ntiles;
+    a.hand_gap = a.hand_bits + a.ntiles;
+    a.bits = d_bits;
+    a.words = words;
+    a.gaps = d_gaps;
+    a.segments = segments;
+    a.gap_words = (segments + 7) / 8;
+    hgap::EncTable t;
+    hgap::make_enc_table(*cb, &t);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(ws, 0, need, st) != cudaSuccess) return HGAP_ERR_CUDA;
+    return cuda_status(hgap::launch_encode(a, t, stream));
+}
+
+size_t hgap_decode_workspace_bytes(uint64_t segments) {
+    return kWsHeader + sizeof(uint64_t) * (size_t)hgap::decode_tiles(segments);
+}
+
+hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps,
+                        uint64_t segments, const hgap_codebook* cb, uint8_t* d_out, uint64_t n,
+                        void* d_workspace, size_t workspace_bytes, hgap_stream_t stream) {
+    if (!cb) return HGAP_ERR_INVALID_ARG;
+    if (n == 0) return (words == 0 && segments == 0) ? HGAP_OK : HGAP_ERR_SIZE;
+    if (!d_bits || !d_gaps || !d_out || !d_workspace) return HGAP_ERR_INVALID_ARG;
+    if (!aligned(d_bits, 4) || !aligned(d_gaps, 4) || !aligned(d_workspace, 8))
+        return HGAP_ERR_INVALID_ARG;
+    if (words == 0 || segments != (words + 3) / 4) return HGAP_ERR_SIZE;
+    hgap_codebook book;
+    hgap_status s = canonical_copy(cb, &book);
+    if (s != HGAP_OK) return s;
+    if (book.symbol_count == 0) return HGAP_ERR_CORRUPT;
+    hgap::DecTable t;
+    s = hgap::make_dec_table(book, &t);
+    if (s != HGAP_OK) return s;
+    hgap::DecArgs a;
+    a.bits = d_bits;
+    a.words = words;
+    a.gaps = d_gaps;
+    a.segments = segments;
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(d_out);
+    a.out_lo = addr & 15;
+    a.out_aligned = reinterpret_cast<uint8_t*>(addr - a.out_lo);
+    a.n = n;
+    a.ntiles = hgap::decode_tiles(segments);
+    if (a.ntiles >= 0xffffffffull) return HGAP_ERR_UNSUPPORTED;
+    const size_t need = kWsHeader + sizeof(uint64_t) * (size_t)a.ntiles;
+    if (workspace_bytes < need) return HGAP_ERR_WORKSPACE;
+    uint8_t* ws = static_cast<uint8_t*>(d_workspace);
+    a.status = reinterpret_cast<uint32_t*>(ws);
+    a.counter = reinterpret_cast<uint32_t*>(ws) + 1;
+    a.lookback = reinterpret_cast<uint64_t*>(ws + kWsHeader);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(ws, 0, need, st) != cudaSuccess) return HGAP_ERR_CUDA;
+    return cuda_status(hgap::launch_decode(a, t, stream));
+}
+
+hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream) {
+    if (!d_workspace) return HGAP_ERR_INVALID_ARG;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t flags = 0;
+    if (cudaMemcpyAsync(&flags, d_workspace, sizeof(flags), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return HGAP_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return HGAP_ERR_CUDA;
+    if (flags & hgap::kDevTimeout) return HGAP_ERR_TIMEOUT;
+    if (flags & hgap::kDevNoCode) return HGAP_ERR_NO_CODE;
+    if (flags & hgap::kDevCorrupt) return HGAP_ERR_CORRUPT;
+    if (flags & hgap::kDevSize) return HGAP_ERR_SIZE;
+    return HGAP_OK;
+}
+
+}  // extern "C"

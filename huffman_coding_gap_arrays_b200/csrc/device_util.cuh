@@ -1,0 +1,116 @@
+// device_util.cuh -- small sm_100a building blocks shared by the kernels:
+// streaming loads, relaxed GPU-scope flag traffic, bounded waits and the
+// warp-wide decoupled look-back.
+#pragma once
+
+#include <cstdint>
+
+#include "hgap_internal.h"
+
+namespace hgap {
+
+constexpr unsigned kFull = 0xffffffffu;
+// A wait gives up after this long (ns of %globaltimer) and flags kDevTimeout.
+constexpr uint64_t kWaitLimitNs = 500ull * 1000 * 1000;
+
+__device__ __forceinline__ uint4 ld_stream_v4(const void* p) {
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint64_t global_timer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits until *p != 0 and returns it.  Bounded: after kWaitLimitNs, or as
+// soon as any error is already flagged, it flags kDevTimeout and returns
+// `fallback`, so the caller finishes its tile and the kernel exits.
+__device__ __forceinline__ uint64_t wait_nonzero(const uint64_t* p, uint32_t* status,
+                                                 uint64_t fallback) {
+    uint64_t v = ld_relaxed_u64(p);
+    if (v != 0) return v;
+    const uint64_t t0 = global_timer_ns();
+    for (uint32_t it = 1;; ++it) {
+        v = ld_relaxed_u64(p);
+        if (v != 0) return v;
+        if ((it & 31) == 0) {
+            if (ld_relaxed_u32(status) != 0 || global_timer_ns() - t0 > kWaitLimitNs) {
+                atomicOr(status, kDevTimeout);
+                return fallback;
+            }
+            __nanosleep(64);
+        }
+    }
+}
+
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(kFull, v, d);
+    return v;
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, uint32_t lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, v, d);
+        if (lane >= (uint32_t)d) v += t;
+    }
+    return v;
+}
+
+// Single-pass decoupled look-back (the reference's scheme,
+// encoder/src/encoder.cu:222-263, decoder/src/decoder.cu:601-638), run by one
+// full warp: publishes the tile aggregate, then inspects 32 predecessors per
+// step, nearest first, until one carries an inclusive prefix.  Every wait is
+// bounded.  Returns the exclusive prefix of `tile` to all lanes and publishes
+// its inclusive prefix.
+__device__ __forceinline__ uint64_t lookback_warp(uint64_t* rec, uint64_t tile, uint64_t agg,
+                                                  uint32_t* status, uint32_t lane) {
+    if (tile == 0) {
+        if (lane == 0) st_relaxed_u64(rec, kFlagP | agg);
+        return 0;
+    }
+    if (lane == 0) st_relaxed_u64(rec + tile, kFlagA | agg);
+    uint64_t excl = 0;
+    int64_t idx = (int64_t)tile - 1 - (int64_t)lane;
+    for (;;) {
+        const uint64_t v = idx >= 0 ? wait_nonzero(rec + idx, status, kFlagP) : kFlagP;
+        const uint32_t pmask = __ballot_sync(kFull, (v & kFlagP) != 0);
+        uint64_t val = v & kValueMask;
+        if (pmask != 0 && lane > (uint32_t)(__ffs(pmask) - 1)) val = 0;
+        excl += warp_sum_u64(val);
+        if (pmask != 0) break;
+        idx -= 32;
+    }
+    if (lane == 0) st_relaxed_u64(rec + tile, kFlagP | ((excl + agg) & kValueMask));
+    return excl;
+}
+
+}  // namespace hgap

@@ -1,0 +1,102 @@
+// hist.cu -- 256-bin byte histogram for sm_100a.
+//
+// Replaces cu_histgram + mergeHistogram (encoder/src/encoder.cu:33-116).
+// Design: one pass, one launch, no scratch.  Each CTA keeps 32 lane-private
+// copies of the 256 counters (h[bin*32 + lane]); lane L only touches bank L,
+// so the shared-memory atomics of a warp never conflict, whatever the byte
+// distribution (the reference's per-warp histograms serialise on skewed data).
+// Input is read as 16-byte streaming loads (virtual 16-byte-aligned chunks;
+// the ragged head/tail chunks are counted byte by byte).  At the end each CTA
+// folds its 32 copies and adds them to the 256 global bins with one atomic
+// per bin.
+#include <cuda_runtime.h>
+
+#include "device_util.cuh"
+
+namespace hgap {
+
+constexpr int kHistThreads = 512;
+constexpr int kHistUnroll = 4;
+
+__device__ __forceinline__ void hist_word(uint32_t* hl, uint32_t w) {
+    atomicAdd(hl + ((w << 5) & 0x1fe0u), 1u);
+    atomicAdd(hl + ((w >> 3) & 0x1fe0u), 1u);
+    atomicAdd(hl + ((w >> 11) & 0x1fe0u), 1u);
+    atomicAdd(hl + ((w >> 19) & 0x1fe0u), 1u);
+}
+
+__device__ __forceinline__ void hist_chunk(uint32_t* hl, const uint4 v) {
+    hist_word(hl, v.x);
+    hist_word(hl, v.y);
+    hist_word(hl, v.z);
+    hist_word(hl, v.w);
+}
+
+__global__ void __launch_bounds__(kHistThreads, 4)
+    hist_kernel(const uint8_t* __restrict__ in_al, uint64_t lo, uint64_t hi,
+                uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[256 * 32];
+    for (int i = threadIdx.x; i < 256 * 32; i += kHistThreads) h[i] = 0;
+    __syncthreads();
+    uint32_t* hl = h + (threadIdx.x & 31);
+
+    const uint64_t first_full = (lo + 15) >> 4;  // chunks wholly inside [lo, hi)
+    const uint64_t end_full = hi >> 4;
+    const uint64_t stride = (uint64_t)gridDim.x * kHistThreads;
+    uint64_t c = first_full + (uint64_t)blockIdx.x * kHistThreads + threadIdx.x;
+    for (; c + (kHistUnroll - 1) * stride < end_full; c += kHistUnroll * stride) {
+        uint4 v[kHistUnroll];
+#pragma unroll
+        for (int u = 0; u < kHistUnroll; ++u) v[u] = ld_stream_v4(in_al + ((c + u * stride) << 4));
+#pragma unroll
+        for (int u = 0; u < kHistUnroll; ++u) hist_chunk(hl, v[u]);
+    }
+    for (; c < end_full; c += stride) hist_chunk(hl, ld_stream_v4(in_al + (c << 4)));
+
+    // ragged head chunk (0, when lo > 0) and tail chunk (hi >> 4, when hi & 15)
+    if (blockIdx.x == 0 && threadIdx.x < 2) {
+        uint64_t q = threadIdx.x == 0 ? 0 : (hi >> 4);
+        const bool is_edge = threadIdx.x == 0 ? (lo != 0) : ((hi & 15) != 0 && (q != 0 || lo == 0));
+        if (is_edge && (q << 4) < hi) {
+            const uint4 v = ld_stream_v4(in_al + (q << 4));
+            const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+            for (uint64_t b = q << 4; b < (q << 4) + 16; ++b) {
+                if (b < lo || b >= hi) continue;
+                const uint32_t byte = (wv[(b & 15) >> 2] >> (8 * (b & 3))) & 0xffu;
+                atomicAdd(hl + (byte << 5), 1u);
+            }
+        }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < 256; b += kHistThreads) {
+        uint32_t s = 0;
+#pragma unroll 8
+        for (int j = 0; j < 32; ++j) s += h[b * 32 + ((j + b) & 31)];
+        if (s) atomicAdd(hist + b, s);
+    }
+}
+
+int launch_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, void* stream) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(d_hist, 0, 256 * sizeof(uint32_t), st);
+    if (e != cudaSuccess || n == 0) return e;
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(d_in);
+    const uint64_t lo = addr & 15;
+    const uint8_t* al = reinterpret_cast<const uint8_t*>(addr - lo);
+    static int sms = 0, per_sm = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hist_kernel, kHistThreads, 0);
+        if (per_sm < 1) per_sm = 1;
+    }
+    const uint64_t chunks = (lo + n + 15) >> 4;
+    uint64_t want = (chunks + (uint64_t)kHistThreads * kHistUnroll - 1) / ((uint64_t)kHistThreads * kHistUnroll);
+    const uint64_t cap = (uint64_t)sms * per_sm;
+    const unsigned grid = (unsigned)(want < 1 ? 1 : (want > cap ? cap : want));
+    hist_kernel<<<grid, kHistThreads, 0, st>>>(al, lo, lo + n, d_hist);
+    return cudaGetLastError();
+}
+
+}  // namespace hgap

@@ -1,0 +1,188 @@
+/*
+ * hgap.h -- C ABI of the B200 Huffman-with-gap-arrays library (libhgap.so).
+ *
+ * Drop-in for the hot path of daisuke-takafuji/Huffman_coding_Gap_arrays:
+ * byte histogram -> length-limited canonical codebook -> bit-packing encoder
+ * that emits the gap array -> segment-parallel decoder, in the reference's
+ * compressed format.  Every entry point names the reference interface it
+ * replaces.  Device entry points are stream-ordered, allocate nothing (the
+ * caller passes a workspace sized by the *_workspace_bytes queries), never
+ * exit the process, and return an hgap_status.
+ *
+ * Format (fixed by the reference, encoder/include/constants.hpp:4-12):
+ *   - codewords of at most 16 bits, canonical, most frequent symbol first;
+ *   - bitstream: u32 words, codes packed MSB first, last word zero-padded;
+ *   - gap array: one 4-bit entry per 128-bit segment, eight per u32, low
+ *     nibble first; entry k = bit offset of the first codeword that starts in
+ *     segment k+1, relative to that segment's start (encoder/src/encoder.cu:307-312).
+ *   - sizes: B code bits, W = ceil(B/32) words, S = ceil(B/128) segments,
+ *     ceil(S/8) gap words (encoder/src/huff.cpp:84-88).
+ */
+#ifndef HGAP_H
+#define HGAP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same type as cudaStream_t (struct CUstream_st*); 0 = the legacy default stream. */
+typedef struct CUstream_st* hgap_stream_t;
+
+typedef enum hgap_status {
+    HGAP_OK = 0,
+    HGAP_ERR_INVALID_ARG = 1,  /* bad pointer, size or alignment */
+    HGAP_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    HGAP_ERR_TIMEOUT = 3,      /* a bounded inter-tile wait expired on the device */
+    HGAP_ERR_CORRUPT = 4,      /* stream, gap array or codebook failed validation */
+    HGAP_ERR_SIZE = 5,         /* sizes disagree (input vs. codebook vs. W/S) */
+    HGAP_ERR_WORKSPACE = 6,    /* workspace too small */
+    HGAP_ERR_NO_CODE = 7,      /* input byte without a codeword */
+    HGAP_ERR_UNSUPPORTED = 8   /* valid request outside this build's limits */
+} hgap_status;
+
+#define HGAP_MAX_CODE_LEN 16
+#define HGAP_SEGMENT_BITS 128
+#define HGAP_GAPS_PER_WORD 8
+
+/* Container entry, reference decoder/src/huff.cpp:45-52 ({u8 symbol, u8 length}). */
+typedef struct hgap_symlen {
+    uint8_t symbol;
+    uint8_t length;
+} hgap_symlen;
+
+/* Reference struct Codetable (encoder/include/constants.hpp:40-43). */
+typedef struct hgap_codeword {
+    uint32_t code;
+    uint32_t length; /* 0 = byte value absent from the book */
+} hgap_codeword;
+
+/* A codebook: the container-order symbol list (most frequent first, as the
+ * reference writes it, encoder/src/huff.cpp:114-119) and the per-byte table. */
+typedef struct hgap_codebook {
+    uint32_t symbol_count;
+    hgap_symlen symbols[256];
+    hgap_codeword table[256];
+} hgap_codebook;
+
+typedef struct hgap_sizes {
+    uint64_t bits;      /* B */
+    uint64_t words;     /* W = ceil(B/32) */
+    uint64_t segments;  /* S = ceil(B/128) */
+    uint64_t gap_words; /* ceil(S/8) */
+} hgap_sizes;
+
+const char* hgap_status_string(hgap_status s);
+
+/* ------------------------------------------------------------------ histogram
+ * Replaces extern "C" histgram(unsigned *d_Histogram, unsigned *d_Data,
+ * unsigned byteCount) (encoder/src/encoder.cu:118-140, decl
+ * encoder/include/encoder.cuh:20-23).  d_in: any alignment; d_hist: 256 u32,
+ * overwritten.  No scratch memory. */
+hgap_status hgap_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, hgap_stream_t stream);
+
+/* ------------------------------------------------------------------- codebook
+ * Replaces store_symbols + qsort(compare) + boundary_PM + get_outputfilesize
+ * (encoder/src/symbols.cpp:29-55, encoder/src/huff.cpp:17-21,77-88,
+ * encoder/src/package_merge.cpp:107-182).  Byte-identical lengths, tie order
+ * and codes.  One distinct symbol gets a 1-bit code (the reference is
+ * undefined there); zero symbols give an empty book.  `sizes` may be NULL. */
+hgap_status hgap_codebook_build(const uint32_t hist[256], hgap_codebook* cb, hgap_sizes* sizes);
+
+/* Rebuilds the canonical codes from a container-order list (the decoder's
+ * view, decoder/src/huff.cpp:140-152).  Rejects non-monotone lengths, lengths
+ * outside 1..16 and over-full (Kraft sum > 1) books. */
+hgap_status hgap_codebook_from_symbols(const hgap_symlen* symbols, uint32_t count,
+                                       hgap_codebook* cb);
+
+hgap_sizes hgap_sizes_from_bits(uint64_t bits);
+
+/* B = sum(len[b] * hist[b]) in 64-bit arithmetic (get_outputfilesize,
+ * encoder/src/symbols.cpp:45-55, whose u32 products overflow for huge counts). */
+uint64_t hgap_encoded_bits(const hgap_codebook* cb, const uint32_t hist[256]);
+
+/* --------------------------------------------------------------------- encode
+ * Replaces void encode(unsigned* outputfile, unsigned outputfilesize,
+ * unsigned* d_inputfile, unsigned inputfilesize, unsigned gap_elements,
+ * Codetable* codetable) (encoder/src/encoder.cu:381-457, decl
+ * encoder/include/encoder.cuh:12-18): device in, device out, no ownership
+ * transfer.  One fused kernel: per-tile code lengths, block scan, bounded
+ * decoupled look-back, packing, gap nibbles; no pre-zeroing of the outputs.
+ * `words` and `segments` are W and S of the stream (hgap_sizes); d_bits gets
+ * W words, d_gaps ceil(S/8) words.  d_in: any alignment; d_bits/d_gaps: 4-byte
+ * aligned.  Device-side errors are reported by hgap_workspace_status(). */
+size_t hgap_encode_workspace_bytes(uint64_t n);
+hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
+                        uint64_t words, uint32_t* d_gaps, uint64_t segments, void* d_workspace,
+                        size_t workspace_bytes, hgap_stream_t stream);
+
+/* --------------------------------------------------------------------- decode
+ * Replaces void decoder_l1_l2(unsigned* input, int inputfilesize,
+ * unsigned* output, int outputfilesize, int gap_elements, void* dectable,
+ * int tablesize, unsigned prefix_bit, unsigned symbol_count, TableInfo)
+ * (decoder/src/decoder.cu:732-815, decl decoder/include/decoder.cuh:4-15):
+ * device in/out, gap array and bitstream as separate pointers, the two-level
+ * table built internally from the codebook (with the correct level-1
+ * boundary, see decoder/src/get_table.cpp:20 for the reference's).  Decodes
+ * each 128-bit segment once, stops at exactly n symbols and checks every
+ * segment's end against the next gap entry.  d_bits/d_gaps: 4-byte aligned;
+ * d_out: any alignment. */
+size_t hgap_decode_workspace_bytes(uint64_t segments);
+hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps,
+                        uint64_t segments, const hgap_codebook* cb, uint8_t* d_out, uint64_t n,
+                        void* d_workspace, size_t workspace_bytes, hgap_stream_t stream);
+
+/* Synchronizes `stream` and returns the device-side status of the last
+ * hgap_encode / hgap_decode that used this workspace (HGAP_OK,
+ * HGAP_ERR_TIMEOUT, HGAP_ERR_CORRUPT, HGAP_ERR_SIZE or HGAP_ERR_NO_CODE). */
+hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream);
+
+/* ------------------------------------------------------------------ container
+ * Writer encoder/src/huff.cpp:111-125, reader decoder/src/huff.cpp:27-81:
+ * u64 symbol_count; symbol_count x {u8 symbol, u8 length}; u32 n; u32 W;
+ * u32 S; u32 gap[ceil(S/8)]; u32 bits[W]; little-endian, unaligned. */
+size_t hgap_container_bytes(uint32_t symbol_count, uint64_t words, uint64_t segments);
+hgap_status hgap_container_write(void* dst, size_t capacity, const hgap_codebook* cb, uint64_t n,
+                                 uint64_t words, uint64_t segments, const uint32_t* gaps,
+                                 const uint32_t* bits, size_t* written);
+/* Parses and validates a container held in host memory; `gaps`/`bits` point
+ * into `src` (unaligned). */
+hgap_status hgap_container_parse(const void* src, size_t size, hgap_codebook* cb, uint64_t* n,
+                                 uint64_t* words, uint64_t* segments, const void** gaps,
+                                 const void** bits);
+
+/* ------------------------------------------------ reference-signature entries
+ * Same arguments and semantics as the reference's own functions, host-side
+ * and synchronous like them, so the reference's bin/encoder and bin/decoder
+ * mains link against this library unchanged (see include/hgap_ref_compat.h
+ * for the C++-linkage forwarders).  Errors print and return instead of
+ * exit(). */
+
+/* encoder/src/encoder.cu:118-140: d_Data holds ceil(byteCount/4) words. */
+void histgram(unsigned int* d_Histogram, unsigned int* d_Data, unsigned int byteCount);
+
+/* encoder/src/encoder.cu:381-457: writes outputfilesize bitstream words then
+ * ceil(gap_array_elements_num/8) gap words into the (pinned) host buffer
+ * outputfile, and frees d_inputfile like the reference (encoder.cu:451). */
+hgap_status hgap_ref_encode(unsigned int* outputfile, unsigned int outputfilesize,
+                            unsigned int* d_inputfile, unsigned int inputfilesize,
+                            unsigned int gap_array_elements_num, const hgap_codeword* codetable);
+
+/* decoder/src/decoder.cu:732-815 minus the 200-iteration timing loop: input =
+ * host gap array followed by the bitstream (inputfilesize words), output =
+ * host buffer of ceil(outputfilesize/4) words.  The reference LUT blob
+ * (decoder/src/get_table.cpp:48-139 layout) is read back into a codebook;
+ * the l1 boundary in tableinfo is ignored (the reference's can be wrong,
+ * get_table.cpp:20) and recomputed. */
+hgap_status hgap_ref_decoder_l1_l2(unsigned int* input, int inputfilesize, unsigned int* output,
+                                   int outputfilesize, int gap_elements_num, const void* dectable,
+                                   int tablesize, unsigned int prefix_bit,
+                                   unsigned int symbol_count, uint32_t l1table_size,
+                                   uint32_t l2table_size, uint32_t ptrtable_size);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HGAP_H */

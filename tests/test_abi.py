@@ -1,0 +1,140 @@
+"""libhgap.so without a GPU: it loads, exports every symbol include/hgap.h
+declares, and its host half (codebook, container, argument checks) matches
+the oracle and the reference's own host code."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import huffman_coding_gap_arrays_b200 as H
+from huffman_coding_gap_arrays_b200 import _lib
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    text = open(os.path.join(ROOT, "include", "hgap.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = set(re.findall(r"\b([A-Za-z_]\w*)\s*\(", text))
+    return sorted(n for n in names if n.startswith("hgap_") or n == "histgram")
+
+
+def test_every_declared_symbol_is_exported():
+    L = _lib.lib()
+    declared = _declared()
+    assert len(declared) >= 15
+    missing = [n for n in declared if not hasattr(L, n)]
+    assert not missing, missing
+    assert sorted(_lib.EXPORTS) == declared
+
+
+def test_status_strings():
+    L = _lib.lib()
+    for s in range(9):
+        assert L.hgap_status_string(s)
+    assert L.hgap_status_string(0) == b"ok"
+
+
+def test_codebook_matches_oracle_and_reference():
+    rng = np.random.default_rng(7)
+    for it in range(500):
+        h = rng.integers(0, 2000, size=256).astype(np.uint32)
+        h[rng.random(256) < rng.random()] = 0
+        if it % 7 == 0:
+            h = np.zeros(256, np.uint32)
+            f = [1, 1]
+            while len(f) < 40:
+                f.append(f[-1] + f[-2])
+            h[rng.choice(256, 40, replace=False)] = f
+        if (h > 0).sum() == 0:
+            continue
+        book, sizes = H.Codebook.from_histogram(h)
+        cb = O.codebook(h)
+        assert np.array_equal(book.symbols, cb.symbols)
+        assert np.array_equal(book.lengths, cb.lengths)
+        assert np.array_equal(book.code, cb.code) and np.array_equal(book.length, cb.length)
+        assert sizes.bits == cb.total_bits
+        if O.ref_available() and (h > 0).sum() >= 2:
+            ref = O.ref_codebook(h)
+            assert np.array_equal(book.lengths, ref.lengths) and np.array_equal(book.code, ref.code)
+
+
+def test_single_symbol_book_is_defined():
+    h = np.zeros(256, np.uint32)
+    h[200] = 12345
+    book, sizes = H.Codebook.from_histogram(h)
+    assert book.symbol_count == 1 and book.length[200] == 1 and book.code[200] == 0
+    assert (sizes.bits, sizes.words, sizes.segments) == (12345, 386, 97)
+
+
+@pytest.mark.parametrize("syms,lens", [
+    ([1, 2, 3], [2, 1, 2]),        # lengths not monotone
+    ([1, 1], [1, 1]),              # duplicate symbol
+    ([1, 2, 3], [1, 1, 1]),        # Kraft sum > 1
+    ([1], [17]),                   # longer than 16 bits
+])
+def test_bad_symbol_lists_rejected(syms, lens):
+    with pytest.raises(H.HgapError):
+        H.Codebook.from_symbols(syms, lens)
+
+
+def test_container_write_matches_oracle_bytes():
+    rng = np.random.default_rng(3)
+    r = np.arange(1, 257); p = r ** -1.2; p /= p.sum()
+    x = rng.choice(256, size=50_000, p=p).astype(np.uint8)
+    h = O.histogram(x)
+    cb = O.codebook(h)
+    bits, gaps, B = O.encode(x, cb)
+    S = (B + 127) // 128
+    expect = O.container(cb, x.size, bits, gaps, S)
+    book, sizes = H.Codebook.from_histogram(h)
+    import torch
+    c = H.Compressed(book, x.size, sizes, torch.from_numpy(bits.view(np.int32)),
+                     torch.from_numpy(gaps.view(np.int32)))
+    blob = c.to_container()
+    assert blob == expect
+    back = H.Compressed.from_container(blob, device="cpu")
+    assert back.n == x.size
+    assert (back.sizes.words, back.sizes.segments, back.sizes.gap_words) == (sizes.words, sizes.segments, sizes.gap_words)
+    assert np.array_equal(back.book.symbols, book.symbols)
+    assert np.array_equal(back.bits.numpy().view(np.uint32), bits)
+    assert np.array_equal(back.gaps.numpy().view(np.uint32), gaps)
+
+
+def test_container_parse_rejects_damage():
+    x = np.frombuffer(b"hello gap arrays " * 40, np.uint8)
+    cb = O.codebook(O.histogram(x))
+    bits, gaps, B = O.encode(x, cb)
+    blob = O.container(cb, x.size, bits, gaps, (B + 127) // 128)
+    for cut in (0, 7, 20, len(blob) - 1):
+        with pytest.raises(H.HgapError):
+            H.Compressed.from_container(blob[:cut], device="cpu")
+    bad = bytearray(blob)
+    bad[0] = 0xFF  # symbol count > 256
+    with pytest.raises(H.HgapError):
+        H.Compressed.from_container(bytes(bad), device="cpu")
+
+
+def test_argument_checks_need_no_gpu():
+    L = _lib.lib()
+    cb = _lib.CCodebook()
+    # n == 0 with W == S == 0 is a no-op; anything else is a size error
+    assert L.hgap_encode(None, 0, C.byref(cb), None, 0, None, 0, None, 0, None) == 0
+    assert L.hgap_encode(None, 0, C.byref(cb), None, 1, None, 1, None, 0, None) == 5
+    assert L.hgap_encode(None, 10, C.byref(cb), None, 1, None, 1, None, 0, None) == 1
+    assert L.hgap_decode(None, 0, None, 0, C.byref(cb), None, 0, None, 0, None) == 0
+    assert L.hgap_decode(None, 3, None, 1, C.byref(cb), None, 10, None, 0, None) == 1
+    assert L.hgap_histogram(None, 10, None, None) == 1
+    # workspace sizes grow with the input
+    assert L.hgap_encode_workspace_bytes(1 << 30) > L.hgap_encode_workspace_bytes(1 << 20)
+    assert L.hgap_decode_workspace_bytes(1 << 20) > L.hgap_decode_workspace_bytes(1 << 10)
+
+
+def test_encoded_bits_is_64bit():
+    h = np.zeros(256, np.uint32)
+    h[:3] = [3_000_000_000, 2_900_000_000, 1_000_000_000]
+    book, sizes = H.Codebook.from_histogram(h)
+    assert sizes.bits == sum(int(book.length[b]) * int(h[b]) for b in range(3))
