@@ -25,7 +25,7 @@ EXPORTS = [
     "hgap_sizes_from_bits", "hgap_encoded_bits", "hgap_encode_workspace_bytes", "hgap_encode",
     "hgap_decode_workspace_bytes", "hgap_decode", "hgap_workspace_status", "hgap_container_bytes",
     "hgap_container_write", "hgap_container_parse", "histgram", "hgap_ref_encode",
-    "hgap_ref_decoder_l1_l2",
+    "hgap_ref_decoder_l1_l2", "hgap_decode_noalloc",
 ]
 
 
@@ -81,6 +81,7 @@ def lib() -> C.CDLL:
     L.hgap_decode_workspace_bytes.restype = C.c_size_t
     L.hgap_decode.argtypes = [vp, u64, vp, u64, C.POINTER(CCodebook), vp, u64, vp, C.c_size_t, vp]
     L.hgap_workspace_status.argtypes = [vp, vp]
+    L.hgap_decode_noalloc.argtypes = [vp, u64, vp, u64, C.POINTER(CCodebook), vp, u64, vp]
     L.hgap_container_bytes.argtypes = [C.c_uint32, u64, u64]
     L.hgap_container_bytes.restype = C.c_size_t
     L.hgap_container_write.argtypes = [vp, C.c_size_t, C.POINTER(CCodebook), u64, u64, u64, vp, vp,
@@ -94,7 +95,8 @@ def lib() -> C.CDLL:
                                          C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
     for name in ("hgap_histogram", "hgap_codebook_build", "hgap_codebook_from_symbols",
                  "hgap_encode", "hgap_decode", "hgap_workspace_status", "hgap_container_write",
-                 "hgap_container_parse", "hgap_ref_encode", "hgap_ref_decoder_l1_l2"):
+                 "hgap_container_parse", "hgap_ref_encode", "hgap_ref_decoder_l1_l2",
+                 "hgap_decode_noalloc"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -139,6 +139,26 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
  * HGAP_ERR_TIMEOUT, HGAP_ERR_CORRUPT, HGAP_ERR_SIZE or HGAP_ERR_NO_CODE). */
 hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream);
 
+/* ------------------------------------------------- decode without allocation
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory at all (code inside a framework that owns every
+ * device allocation through its own pool, plugins barred from allocating on
+ * the hot path, language bindings that only pass the input and output
+ * buffers).  Same arguments and results as hgap_decode minus the workspace:
+ * the decoder's scratch is a fixed HGAP_NOALLOC_SCRATCH_BYTES array inside
+ * libhgap.so, held by every GPU that loads the library until exit.  Streams
+ * with hgap_decode_workspace_bytes(segments) > HGAP_NOALLOC_SCRATCH_BYTES are
+ * rejected with HGAP_ERR_WORKSPACE before anything runs.  The call waits for
+ * `stream` and returns the device-side status too.  The first call on each
+ * device looks up the array's device address; make it before any stream
+ * capture.  All calls share the one array: calls that overlap on the GPU
+ * (other streams, other host threads) race and must be serialized by the
+ * caller.  Allocates nothing. */
+#define HGAP_NOALLOC_SCRATCH_BYTES (256u * 1024u)
+hgap_status hgap_decode_noalloc(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps,
+                                uint64_t segments, const hgap_codebook* cb, uint8_t* d_out,
+                                uint64_t n, hgap_stream_t stream);
+
 /* ------------------------------------------------------------------ container
  * Writer encoder/src/huff.cpp:111-125, reader decoder/src/huff.cpp:27-81:
  * u64 symbol_count; symbol_count x {u8 symbol, u8 length}; u32 n; u32 W;
