@@ -220,14 +220,13 @@ def main():
     hist = torch.empty(256, dtype=torch.int32, device=dev)
     hist_host = torch.empty(256, dtype=torch.int32, pin_memory=True)
 
-    # size the outputs once from the histogram (worst case: 16 bits per byte is
-    # never needed; W for this buffer is fixed)
-    H.histogram(x, out=hist)
+    # size the outputs once from the histogram (W for this buffer is fixed)
+    enc = H.Encoder(n, dev)
+    enc.histogram(x, out=hist)
     book0, sizes0 = H.Codebook.from_histogram(hist.cpu())
     bits = torch.empty(sizes0.words + 16, dtype=torch.int32, device=dev)
     gaps = torch.empty(sizes0.gap_words + 16, dtype=torch.int32, device=dev)
     out = torch.empty(n + 16, dtype=torch.uint8, device=dev)
-    enc = H.Encoder(n, dev)
     dec = H.Decoder(sizes0.segments, dev)
 
     ev = {k: [] for k in ("hist", "encode", "decode")}
@@ -236,7 +235,7 @@ def main():
         e = [torch.cuda.Event(enable_timing=True) for _ in range(6)] if record else None
         if record:
             e[0].record(stream)
-        H.histogram(x, out=hist)
+        enc.histogram(x, out=hist)  # hgap_encode_histogram: global + per-super-tile histograms
         if record:
             e[1].record(stream)
         hist_host.copy_(hist, non_blocking=True)
@@ -244,7 +243,7 @@ def main():
         book, sizes = H.Codebook.from_histogram(hist_host)
         if record:
             e[2].record(stream)
-        enc.encode(x, book, sizes, bits=bits, gaps=gaps, check_status=False)
+        enc.encode(x, book, sizes, bits=bits, gaps=gaps, check_status=False, prepared=True)
         if record:
             e[3].record(stream)
             e[4].record(stream)
@@ -319,11 +318,11 @@ def main():
 
         def e2e_step():
             x_dev.copy_(x_host, non_blocking=True)                      # H2D input
-            H.histogram(x_dev, out=hist)
+            enc.histogram(x_dev, out=hist)
             hist_host.copy_(hist, non_blocking=True)
             stream.synchronize()
             book, sz = H.Codebook.from_histogram(hist_host)
-            b, g = enc.encode(x_dev, book, sz, bits=bits, gaps=gaps, check_status=False)
+            b, g = enc.encode(x_dev, book, sz, bits=bits, gaps=gaps, check_status=False, prepared=True)
             bits_host[:sz.words].copy_(b, non_blocking=True)            # D2H container payload
             gaps_host[:sz.gap_words].copy_(g, non_blocking=True)
             bits_in[:sz.words].copy_(bits_host[:sz.words], non_blocking=True)   # H2D for decode

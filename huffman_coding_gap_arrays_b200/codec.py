@@ -150,8 +150,27 @@ class Encoder:
         nbytes = lib().hgap_encode_workspace_bytes(max(self.capacity, 1))
         self.workspace = torch.empty((nbytes + 7) // 8, dtype=torch.int64, device=dev)
 
+    def histogram(self, x: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """The encoder's histogram pass (hgap_encode_histogram): the global
+        histogram, plus per-super-tile histograms kept in this workspace for a
+        following ``encode(..., prepared=True)`` of the same tensor."""
+        _require_cuda(x, "x")
+        n = x.numel() * x.element_size()
+        if n > self.capacity:
+            raise ValueError(f"input of {n} bytes exceeds encoder capacity {self.capacity}")
+        if out is None:
+            out = torch.empty(256, dtype=torch.int32, device=x.device)
+        ws = self.workspace
+        check(lib().hgap_encode_histogram(x.data_ptr(), n, out.data_ptr(), ws.data_ptr(), ws.numel() * 8,
+                                          _stream(stream)), "hgap_encode_histogram")
+        return out
+
     def encode(self, x: torch.Tensor, book: Codebook, sizes: StreamSizes, bits: torch.Tensor | None = None,
-               gaps: torch.Tensor | None = None, stream=None, check_status: bool = True):
+               gaps: torch.Tensor | None = None, stream=None, check_status: bool = True,
+               prepared: bool = False):
+        """Encode x.  With prepared=True the per-super-tile histograms from the
+        last ``histogram(x)`` on this encoder are reused (one pass over x);
+        otherwise the encoder makes them itself (two passes)."""
         _require_cuda(x, "x")
         n = x.numel() * x.element_size()
         if n > self.capacity:
@@ -161,9 +180,10 @@ class Encoder:
         if gaps is None:
             gaps = torch.empty(max(sizes.gap_words, 1), dtype=torch.int32, device=x.device)
         ws = self.workspace
-        check(lib().hgap_encode(x.data_ptr(), n, C.byref(book.cstruct), bits.data_ptr(), sizes.words,
-                                gaps.data_ptr(), sizes.segments, ws.data_ptr(),
-                                ws.numel() * 8, _stream(stream)), "hgap_encode")
+        fn = lib().hgap_encode_prepared if prepared else lib().hgap_encode
+        check(fn(x.data_ptr(), n, C.byref(book.cstruct), bits.data_ptr(), sizes.words,
+                 gaps.data_ptr(), sizes.segments, ws.data_ptr(), ws.numel() * 8, _stream(stream)),
+              "hgap_encode")
         if check_status:
             self.check(stream)
         return bits[:sizes.words], gaps[:sizes.gap_words]
@@ -249,12 +269,14 @@ def compress(x: torch.Tensor, stream=None) -> Compressed:
     _require_cuda(x, "x")
     x = x.reshape(-1).view(torch.uint8) if x.dtype != torch.uint8 else x.reshape(-1)
     n = x.numel()
-    hist = histogram(x, stream=stream)
-    book, sizes = Codebook.from_histogram(hist.cpu())
     if n == 0:
+        book, sizes = Codebook.from_histogram(np.zeros(256, np.uint32))
         empty = torch.empty(0, dtype=torch.int32, device=x.device)
         return Compressed(book, 0, sizes, empty, empty)
-    bits, gaps = Encoder(n, x.device).encode(x, book, sizes, stream=stream)
+    enc = Encoder(n, x.device)
+    hist = enc.histogram(x, stream=stream)
+    book, sizes = Codebook.from_histogram(hist.cpu())
+    bits, gaps = enc.encode(x, book, sizes, stream=stream, prepared=True)
     return Compressed(book, n, sizes, bits, gaps)
 
 

@@ -31,7 +31,109 @@ hgap_status hgap_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, hgap_
 }
 
 size_t hgap_encode_workspace_bytes(uint64_t n) {
-    return kWsHeader + 3 * sizeof(uint64_t) * (size_t)hgap::encode_tiles(n);
+    const uint64_t nst = hgap::encode_super_tiles(n + 15, n);  // worst case over alignments
+    return hgap::kEncWsHeader + (size_t)nst * (sizeof(uint64_t) + 256 * sizeof(uint32_t));
+}
+
+}  // extern "C"
+
+namespace {
+
+// Carves the encoder workspace for input (d_in, n):
+// [status][counter][..][tag @16][scratch hist @1024][st_rec @2048][st_hist].
+hgap_status encode_layout(const void* d_in, uint64_t n, void* d_workspace, size_t workspace_bytes,
+                          hgap::EncArgs* a, hgap::HistStArgs* h) {
+    if (!d_in || !d_workspace || !aligned(d_workspace, 16)) return HGAP_ERR_INVALID_ARG;
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(d_in);
+    const uint64_t lo = addr & 15;
+    const uint64_t st_bytes = hgap::encode_st_chunks(n) * hgap::kEncChunkBytes;
+    const uint64_t nst = hgap::encode_super_tiles(lo + n, n);
+    if (nst >= 0xffffffffull) return HGAP_ERR_UNSUPPORTED;
+    const size_t need = hgap::kEncWsHeader + (size_t)nst * (sizeof(uint64_t) + 256 * sizeof(uint32_t));
+    if (workspace_bytes < need) return HGAP_ERR_WORKSPACE;
+    uint8_t* ws = static_cast<uint8_t*>(d_workspace);
+    a->in_aligned = reinterpret_cast<const uint8_t*>(addr - lo);
+    a->lo = lo;
+    a->hi = lo + n;
+    a->status = reinterpret_cast<uint32_t*>(ws);
+    a->counter = reinterpret_cast<uint32_t*>(ws) + 1;
+    a->tag = reinterpret_cast<const uint64_t*>(ws + hgap::kEncWsTag);
+    a->st_rec = reinterpret_cast<uint64_t*>(ws + hgap::kEncWsHeader);
+    a->st_hist = reinterpret_cast<const uint32_t*>(a->st_rec + nst);
+    a->nst = nst;
+    a->st_bytes = (uint32_t)st_bytes;
+    h->in_aligned = a->in_aligned;
+    h->lo = lo;
+    h->hi = lo + n;
+    h->hist = reinterpret_cast<uint32_t*>(ws + hgap::kEncWsScratchHist);
+    h->st_hist = const_cast<uint32_t*>(a->st_hist);
+    h->tag = reinterpret_cast<uint64_t*>(ws + hgap::kEncWsTag);
+    h->nst = nst;
+    h->st_bytes = (uint32_t)st_bytes;
+    return HGAP_OK;
+}
+
+hgap_status encode_outputs(const hgap_codebook* cb, uint32_t* d_bits, uint64_t words, uint32_t* d_gaps,
+                           uint64_t segments, hgap::EncArgs* a) {
+    if (!d_bits || !d_gaps || !aligned(d_bits, 4) || !aligned(d_gaps, 4)) return HGAP_ERR_INVALID_ARG;
+    if (segments != (words + 3) / 4 || words == 0) return HGAP_ERR_SIZE;
+    for (int b = 0; b < 256; ++b) {
+        const uint32_t l = cb->table[b].length;
+        if (l > (uint32_t)hgap::kMaxLen || (l && (cb->table[b].code >> l) != 0)) return HGAP_ERR_CORRUPT;
+    }
+    a->bits = d_bits;
+    a->words = words;
+    a->gaps = d_gaps;
+    a->segments = segments;
+    a->gap_words = (segments + 7) / 8;
+    a->bits_aligned16 = aligned(d_bits, 16) ? 1u : 0u;
+    return HGAP_OK;
+}
+
+// Clears status + counter, and the super-tile look-back records.
+hgap_status encode_clear(const hgap::EncArgs& a, bool tag_too, cudaStream_t st) {
+    uint8_t* ws = reinterpret_cast<uint8_t*>(a.status);
+    if (cudaMemsetAsync(ws, 0, tag_too ? hgap::kEncWsHeader : hgap::kEncWsTag, st) != cudaSuccess)
+        return HGAP_ERR_CUDA;
+    if (cudaMemsetAsync(a.st_rec, 0, sizeof(uint64_t) * a.nst, st) != cudaSuccess) return HGAP_ERR_CUDA;
+    return HGAP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+hgap_status hgap_encode_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, void* d_workspace,
+                                  size_t workspace_bytes, hgap_stream_t stream) {
+    if (!d_hist) return HGAP_ERR_INVALID_ARG;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    if (n == 0) return cudaMemsetAsync(d_hist, 0, 1024, st) == cudaSuccess ? HGAP_OK : HGAP_ERR_CUDA;
+    hgap::EncArgs a;
+    hgap::HistStArgs h;
+    hgap_status s = encode_layout(d_in, n, d_workspace, workspace_bytes, &a, &h);
+    if (s != HGAP_OK) return s;
+    h.hist = d_hist;
+    s = encode_clear(a, true, st);
+    if (s != HGAP_OK) return s;
+    return cuda_status(hgap::launch_hist_st(h, stream));
+}
+
+hgap_status hgap_encode_prepared(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
+                                 uint64_t words, uint32_t* d_gaps, uint64_t segments, void* d_workspace,
+                                 size_t workspace_bytes, hgap_stream_t stream) {
+    if (!cb) return HGAP_ERR_INVALID_ARG;
+    if (n == 0) return (words == 0 && segments == 0) ? HGAP_OK : HGAP_ERR_SIZE;
+    hgap::EncArgs a;
+    hgap::HistStArgs h;
+    hgap_status s = encode_layout(d_in, n, d_workspace, workspace_bytes, &a, &h);
+    if (s == HGAP_OK) s = encode_outputs(cb, d_bits, words, d_gaps, segments, &a);
+    if (s != HGAP_OK) return s;
+    hgap::EncTable t;
+    hgap::make_enc_table(*cb, &t);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    s = encode_clear(a, false, st);
+    if (s != HGAP_OK) return s;
+    return cuda_status(hgap::launch_encode(a, t, stream));
 }
 
 hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
@@ -39,38 +141,18 @@ hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, u
                         size_t workspace_bytes, hgap_stream_t stream) {
     if (!cb) return HGAP_ERR_INVALID_ARG;
     if (n == 0) return (words == 0 && segments == 0) ? HGAP_OK : HGAP_ERR_SIZE;
-    if (!d_in || !d_bits || !d_gaps || !d_workspace) return HGAP_ERR_INVALID_ARG;
-    if (!aligned(d_bits, 4) || !aligned(d_gaps, 4) || !aligned(d_workspace, 8))
-        return HGAP_ERR_INVALID_ARG;
-    if (segments != (words + 3) / 4 || words == 0) return HGAP_ERR_SIZE;
-    for (int b = 0; b < 256; ++b) {
-        const uint32_t l = cb->table[b].length;
-        if (l > (uint32_t)hgap::kMaxLen || (l && (cb->table[b].code >> l) != 0)) return HGAP_ERR_CORRUPT;
-    }
-    const uintptr_t addr = reinterpret_cast<uintptr_t>(d_in);
     hgap::EncArgs a;
-    a.lo = addr & 15;
-    a.hi = a.lo + n;
-    a.in_aligned = reinterpret_cast<const uint8_t*>(addr - a.lo);
-    a.ntiles = (a.hi + hgap::kEncTileBytes - 1) / hgap::kEncTileBytes;
-    if (a.ntiles >= 0xffffffffull) return HGAP_ERR_UNSUPPORTED;
-    const size_t need = kWsHeader + 3 * sizeof(uint64_t) * (size_t)a.ntiles;
-    if (workspace_bytes < need) return HGAP_ERR_WORKSPACE;
-    uint8_t* ws = static_cast<uint8_t*>(d_workspace);
-    a.status = reinterpret_cast<uint32_t*>(ws);
-    a.counter = reinterpret_cast<uint32_t*>(ws) + 1;
-    a.lookback = reinterpret_cast<uint64_t*>(ws + kWsHeader);
-    a.hand_bits = a.lookback + a.ntiles;
-    a.hand_gap = a.hand_bits + a.ntiles;
-    a.bits = d_bits;
-    a.words = words;
-    a.gaps = d_gaps;
-    a.segments = segments;
-    a.gap_words = (segments + 7) / 8;
+    hgap::HistStArgs h;
+    hgap_status s = encode_layout(d_in, n, d_workspace, workspace_bytes, &a, &h);
+    if (s == HGAP_OK) s = encode_outputs(cb, d_bits, words, d_gaps, segments, &a);
+    if (s != HGAP_OK) return s;
     hgap::EncTable t;
     hgap::make_enc_table(*cb, &t);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    if (cudaMemsetAsync(ws, 0, need, st) != cudaSuccess) return HGAP_ERR_CUDA;
+    s = encode_clear(a, true, st);
+    if (s != HGAP_OK) return s;
+    int e = hgap::launch_hist_st(h, stream);  // per-super-tile histograms into the workspace
+    if (e != 0) return HGAP_ERR_CUDA;
     return cuda_status(hgap::launch_encode(a, t, stream));
 }
 
@@ -113,7 +195,10 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     a.lookback = reinterpret_cast<uint64_t*>(ws + kWsHeader);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (cudaMemsetAsync(ws, 0, need, st) != cudaSuccess) return HGAP_ERR_CUDA;
-    return cuda_status(hgap::launch_decode(a, t, stream));
+    uint32_t min_len = hgap::kMaxLen;
+    for (uint32_t i = 0; i < book.symbol_count; ++i)
+        if (book.symbols[i].length < min_len) min_len = book.symbols[i].length;
+    return cuda_status(hgap::launch_decode(a, t, min_len, stream));
 }
 
 hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream) {
@@ -127,6 +212,7 @@ hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream)
     if (flags & hgap::kDevNoCode) return HGAP_ERR_NO_CODE;
     if (flags & hgap::kDevCorrupt) return HGAP_ERR_CORRUPT;
     if (flags & hgap::kDevSize) return HGAP_ERR_SIZE;
+    if (flags & hgap::kDevPlan) return HGAP_ERR_INVALID_ARG;
     return HGAP_OK;
 }
 

@@ -113,4 +113,51 @@ __device__ __forceinline__ uint64_t lookback_warp(uint64_t* rec, uint64_t tile, 
     return excl;
 }
 
+// The same look-back with a window of 32*K predecessors per round trip: lane
+// l inspects tiles top-K*l ... top-K*l-K+1 (nearest first).  The inclusive-
+// prefix frontier can advance only one window per L2 round trip, so the window
+// must exceed (tiles started per round trip); at the decoder's tile rate on a
+// B200 a 32-record window would cap the whole kernel.
+template <int K>
+__device__ __forceinline__ uint64_t lookback_warp_wide(uint64_t* rec, uint64_t tile, uint64_t agg,
+                                                       uint32_t* status, uint32_t lane) {
+    if (tile == 0) {
+        if (lane == 0) st_relaxed_u64(rec, kFlagP | agg);
+        return 0;
+    }
+    if (lane == 0) st_relaxed_u64(rec + tile, kFlagA | agg);
+    uint64_t excl = 0;
+    int64_t top = (int64_t)tile - 1;
+    for (;;) {
+        uint64_t v[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const int64_t i = top - (int64_t)(K * lane + j);
+            v[j] = i >= 0 ? ld_relaxed_u64(rec + i) : kFlagP;
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const int64_t i = top - (int64_t)(K * lane + j);
+            if (v[j] == 0) v[j] = wait_nonzero(rec + i, status, kFlagP);
+        }
+        int first = K;  // nearest record of this lane with an inclusive prefix
+#pragma unroll
+        for (int j = K - 1; j >= 0; --j)
+            if (v[j] & kFlagP) first = j;
+        const uint32_t pmask = __ballot_sync(kFull, first < K);
+        const int fl = pmask ? __ffs(pmask) - 1 : 32;
+        uint64_t sum = 0;
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const bool take = (int)lane < fl || ((int)lane == fl && j <= first);
+            if (take) sum += v[j] & kValueMask;
+        }
+        excl += warp_sum_u64(sum);
+        if (pmask) break;
+        top -= 32 * K;
+    }
+    if (lane == 0) st_relaxed_u64(rec + tile, kFlagP | ((excl + agg) & kValueMask));
+    return excl;
+}
+
 }  // namespace hgap

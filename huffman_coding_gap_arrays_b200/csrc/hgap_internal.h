@@ -20,6 +20,7 @@ enum : uint32_t {
     kDevCorrupt = 2u,   // decoder: invalid codeword / segment end != next gap
     kDevNoCode = 4u,    // encoder: an input byte has no codeword
     kDevSize = 8u,      // total bits / symbols disagree with W, S or n
+    kDevPlan = 16u,     // encoder: workspace histograms are not this input's
 };
 
 // Look-back record: 2 flag bits over a 62-bit value (aggregate or inclusive
@@ -43,7 +44,33 @@ struct EncTable {
 };
 constexpr uint32_t kEncAbsent = 0x80000000u;
 
-constexpr int kEncTileBytes = 8192;  // input bytes per encoder tile
+// The encoder works on super-tiles: `st_chunks` chunks of kEncChunkBytes input
+// bytes each.  The histogram pass that precedes it also records one 256-bin
+// histogram per super-tile, so a super-tile's bit count -- and, after one
+// look-back over super-tiles, its first output bit -- is known before any of
+// its bytes are encoded.  st_chunks depends on n only (hgap_internal
+// encode_st_chunks), so both passes and the workspace query agree.
+constexpr int kEncChunkBytes = 8192;
+constexpr int kEncMaxStChunks = 32;
+constexpr uint64_t kEncTargetSuperTiles = 2368;  // ~16 per SM on a 148-SM B200
+
+// Encoder workspace: [status u32][counter u32][pad][tag: n u64, input u64] ...
+// [scratch histogram u32 x 256 at 1024] [st_rec u64 x nst at 2048] [st_hist u32 x 256 x nst]
+constexpr size_t kEncWsHeader = 2048;
+constexpr size_t kEncWsTag = 16;
+constexpr size_t kEncWsScratchHist = 1024;
+
+inline uint64_t encode_st_chunks(uint64_t n) {
+    const uint64_t chunks = (n + 15 + kEncChunkBytes - 1) / kEncChunkBytes;
+    uint64_t c = (chunks + kEncTargetSuperTiles - 1) / kEncTargetSuperTiles;
+    if (c < 1) c = 1;
+    if (c > (uint64_t)kEncMaxStChunks) c = kEncMaxStChunks;
+    return c;
+}
+inline uint64_t encode_super_tiles(uint64_t lo_plus_n, uint64_t n) {
+    const uint64_t st = encode_st_chunks(n) * kEncChunkBytes;
+    return (lo_plus_n + st - 1) / st;
+}
 
 struct EncArgs {
     const uint8_t* in_aligned;  // input rounded down to 16 bytes
@@ -54,12 +81,24 @@ struct EncArgs {
     uint32_t* gaps;
     uint64_t gap_words;
     uint64_t segments;
-    uint64_t* lookback;  // [ntiles]
-    uint64_t* hand_bits; // [ntiles] partial last bitstream word of each tile
-    uint64_t* hand_gap;  // [ntiles] partial last gap word of each tile
+    uint64_t* st_rec;          // [nst] look-back records over super-tiles
+    const uint32_t* st_hist;   // [nst][256] per-super-tile histograms
+    const uint64_t* tag;       // {n, input address} written by the histogram pass
     uint32_t* counter;
     uint32_t* status;
-    uint64_t ntiles;
+    uint64_t nst;
+    uint32_t st_bytes;         // super-tile size in input bytes
+    uint32_t bits_aligned16;   // d_bits is 16-byte aligned: vector stores allowed
+};
+
+struct HistStArgs {
+    const uint8_t* in_aligned;
+    uint64_t lo, hi;
+    uint32_t* hist;      // [256] global histogram (zeroed by the launcher)
+    uint32_t* st_hist;   // [nst][256]
+    uint64_t* tag;       // receives {n, input address}
+    uint64_t nst;
+    uint32_t st_bytes;
 };
 
 // ---------------------------------------------------------------- decoder ---
@@ -93,8 +132,8 @@ struct DecArgs {
 // Implemented in the .cu files; return cudaError_t as int.
 int launch_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, void* stream);
 int launch_encode(const EncArgs& a, const EncTable& t, void* stream);
-int launch_decode(const DecArgs& a, const DecTable& t, void* stream);
-uint64_t encode_tiles(uint64_t n);          // tiles for an n-byte input (any alignment)
+int launch_hist_st(const HistStArgs& a, void* stream);
+int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, void* stream);
 uint64_t decode_tiles(uint64_t segments);
 
 // ------------------------------------------------------------- host helpers -

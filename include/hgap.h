@@ -108,12 +108,30 @@ uint64_t hgap_encoded_bits(const hgap_codebook* cb, const uint32_t hist[256]);
  * unsigned* d_inputfile, unsigned inputfilesize, unsigned gap_elements,
  * Codetable* codetable) (encoder/src/encoder.cu:381-457, decl
  * encoder/include/encoder.cuh:12-18): device in, device out, no ownership
- * transfer.  One fused kernel: per-tile code lengths, block scan, bounded
- * decoupled look-back, packing, gap nibbles; no pre-zeroing of the outputs.
- * `words` and `segments` are W and S of the stream (hgap_sizes); d_bits gets
- * W words, d_gaps ceil(S/8) words.  d_in: any alignment; d_bits/d_gaps: 4-byte
- * aligned.  Device-side errors are reported by hgap_workspace_status(). */
+ * transfer, no pre-zeroing of the outputs.  `words` and `segments` are W and
+ * S of the stream (hgap_sizes); d_bits gets W words, d_gaps ceil(S/8) words.
+ * d_in: any alignment; d_bits/d_gaps: 4-byte aligned (16 for vector stores);
+ * d_workspace: 16-byte aligned, hgap_encode_workspace_bytes(n) bytes.
+ * Device-side errors are reported by hgap_workspace_status().
+ *
+ * The encoder cuts the input into super-tiles and needs each one's byte
+ * histogram; the pipeline the reference runs (histgram, then encode,
+ * encoder/src/huff.cpp:70-99) therefore maps to two calls that read the input
+ * once each:
+ *   hgap_encode_histogram  -- replaces histgram() in that pipeline: the global
+ *                             histogram into d_hist AND the per-super-tile
+ *                             histograms into the workspace;
+ *   hgap_encode_prepared   -- the encoder proper, reusing them (same input,
+ *                             same workspace; otherwise HGAP_ERR_INVALID_ARG
+ *                             from hgap_workspace_status).
+ * hgap_encode does both passes itself, for callers that only have the codebook. */
 size_t hgap_encode_workspace_bytes(uint64_t n);
+hgap_status hgap_encode_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, void* d_workspace,
+                                  size_t workspace_bytes, hgap_stream_t stream);
+hgap_status hgap_encode_prepared(const void* d_in, uint64_t n, const hgap_codebook* cb,
+                                 uint32_t* d_bits, uint64_t words, uint32_t* d_gaps,
+                                 uint64_t segments, void* d_workspace, size_t workspace_bytes,
+                                 hgap_stream_t stream);
 hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
                         uint64_t words, uint32_t* d_gaps, uint64_t segments, void* d_workspace,
                         size_t workspace_bytes, hgap_stream_t stream);
@@ -136,7 +154,9 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
 
 /* Synchronizes `stream` and returns the device-side status of the last
  * hgap_encode / hgap_decode that used this workspace (HGAP_OK,
- * HGAP_ERR_TIMEOUT, HGAP_ERR_CORRUPT, HGAP_ERR_SIZE or HGAP_ERR_NO_CODE). */
+ * HGAP_ERR_TIMEOUT, HGAP_ERR_CORRUPT, HGAP_ERR_SIZE, HGAP_ERR_NO_CODE, or
+ * HGAP_ERR_INVALID_ARG when hgap_encode_prepared got a workspace that was not
+ * prepared by hgap_encode_histogram on the same input). */
 hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream);
 
 /* ------------------------------------------------- decode without allocation

@@ -243,3 +243,32 @@ def test_ref_encode_and_decode_compat(cuda):
                                   blob.ctypes.data, blob.size, p, cb.count, *info)
     assert rc == 0
     assert np.array_equal(dec.view(np.uint8)[:x.size], x)
+
+
+# ------------------------------------------- encoder histogram pass + prepared
+
+@pytest.mark.parametrize("n,off", [(1, 0), (1000, 3), (1 << 20, 0), (5 * (1 << 20) + 3, 9),
+                                   (40 * (1 << 20) + 5, 1)])
+def test_encode_histogram_then_prepared(cuda, n, off):
+    x = make("zipf" if n % 2 else "uniform", n, n)
+    d = to_dev(x, off)
+    enc = H.Encoder(n)
+    hist = enc.histogram(d)
+    h = O.histogram(x)
+    assert np.array_equal(u32(hist), h)
+    book, sizes = H.Codebook.from_histogram(u32(hist))
+    bits, gaps = enc.encode(d, book, sizes, prepared=True)
+    bits_o, gaps_o, _ = O.encode(x, O.codebook(h))
+    assert np.array_equal(u32(bits), bits_o) and np.array_equal(u32(gaps), gaps_o)
+
+
+def test_prepared_with_foreign_workspace_is_rejected(cuda):
+    x = make("zipf", 300_000, 1)
+    y = make("zipf", 300_000, 2)
+    enc = H.Encoder(x.size)
+    dx, dy = to_dev(x), to_dev(y)
+    enc.histogram(dx)
+    book, sizes = H.Codebook.from_histogram(O.histogram(y))
+    with pytest.raises(H.HgapError) as e:
+        enc.encode(dy, book, sizes, prepared=True)   # histograms belong to x, not y
+    assert e.value.status == 1  # HGAP_ERR_INVALID_ARG
