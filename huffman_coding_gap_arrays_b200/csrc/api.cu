@@ -181,6 +181,7 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     a.words = words;
     a.gaps = d_gaps;
     a.segments = segments;
+    a.gap_words = (segments + 7) / 8;
     const uintptr_t addr = reinterpret_cast<uintptr_t>(d_out);
     a.out_lo = addr & 15;
     a.out_aligned = reinterpret_cast<uint8_t*>(addr - a.out_lo);

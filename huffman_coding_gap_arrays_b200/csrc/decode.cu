@@ -35,18 +35,22 @@ struct DecCfg {
     static constexpr int kMaxSym = 4 * R;
     static constexpr int kWarps = kDecThreads / 32;
     static constexpr int kT1 = 1 << kDecPrefix;        // u32 level-1 entries
-    static constexpr int kT2 = kDecT2Cap;              // u32 level-2 entries
-    static constexpr int kWords = 4 * kDecSegs + 8;
+    static constexpr int kT2 = kDecT2Cap;              // u16 level-2 entries
+    static constexpr int kWords = 4 * kDecSegs + 8;    // bitstream words staged per tile
     static constexpr int kWordsPad = (kWords + kWords / 8 + 8 + 3) & ~3;
-    static constexpr int kStage = kDecSegs * R;        // words: bytes [row][segment]
-    static constexpr int kCompact = (kDecSegs * kMaxSym + 64) / 4;
-    static constexpr size_t kSmem = (size_t)(kT1 + kT2 + kWordsPad + kStage + kCompact) * 4;
-    static_assert(kT1 % 4 == 0 && kT2 % 4 == 0 && kWordsPad % 4 == 0 && kStage % 4 == 0,
-                  "16-byte aligned areas");
+    static constexpr int kWordsPer = (kWords + kDecThreads - 1) / kDecThreads;
+    static constexpr int kGapStage = kDecSegs / 8 + 4;  // gap words of the tile (+1 before)
+    static constexpr int kPitch = kDecSegs + 4;        // stage row pitch (bytes): rows skew banks
+    static constexpr int kStageBytes = kMaxSym * kPitch;
+    static constexpr int kCompactBytes = kDecSegs * kMaxSym + 64;
+    static constexpr size_t kSmem = (size_t)(kT1 + kT2 / 2 + kWordsPad + kGapStage) * 4 +
+                                    kStageBytes + kCompactBytes;
+    static_assert(kT1 % 4 == 0 && (kT2 / 2) % 4 == 0 && kWordsPad % 4 == 0 && kGapStage % 4 == 0 &&
+                  kStageBytes % 16 == 0, "16-byte aligned areas");
 };
 
-// Shared-memory table entry (u32): direct = len << 8 | symbol; pointer =
-// bit 31 | extra width << 16 | level-2 offset; invalid = bit 30.
+// Level-1 table entry in shared memory (u32): direct = len << 8 | symbol;
+// pointer = bit 31 | extra width << 16 | level-2 offset; invalid = bit 30.
 __device__ __forceinline__ uint32_t widen_entry(uint32_t e) {
     if (e & 0x8000u) return 0x80000000u | (((e >> 12) & 7u) << 16) | (e & 0xfffu);
     if (e & kDecInvalid) return 0x40000000u;
@@ -55,8 +59,18 @@ __device__ __forceinline__ uint32_t widen_entry(uint32_t e) {
 
 __device__ __forceinline__ uint32_t pidx(uint32_t w) { return w + (w >> 3); }
 
-__device__ __forceinline__ uint32_t gap_entry(const uint32_t* gaps, uint64_t k) {
-    return (__ldg(gaps + (k >> 3)) >> (4 * (uint32_t)(k & 7))) & 0xfu;
+// One codeword of a segment: window from two staged words, level-1 lookup,
+// level 2 for the rare longer codes.  Returns the widened entry.
+__device__ __forceinline__ uint32_t lookup(const uint32_t* sw, const uint32_t* t1,
+                                           const uint16_t* t2, uint32_t pos) {
+    const uint32_t w = pos >> 5;
+    const uint32_t x = __funnelshift_l(sw[pidx(w + 1)], sw[pidx(w)], pos);
+    uint32_t e = t1[x >> (32 - kDecPrefix)];
+    if (e & 0x80000000u) {
+        const uint32_t wd = (e >> 16) & 7u;
+        e = widen_entry(t2[(e & 0xffffu) + ((x << kDecPrefix) >> (32 - wd))]);
+    }
+    return e;
 }
 
 template <int R>
@@ -65,126 +79,189 @@ __global__ void __launch_bounds__(kDecThreads, 3)
     using C = DecCfg<R>;
     extern __shared__ __align__(16) uint32_t smem[];
     uint32_t* t1 = smem;
-    uint32_t* t2 = t1 + C::kT1;
-    uint32_t* sw = t2 + C::kT2;
-    uint8_t* stage = reinterpret_cast<uint8_t*>(sw + C::kWordsPad);
-    uint32_t* compact = sw + C::kWordsPad + C::kStage;
+    uint16_t* t2 = reinterpret_cast<uint16_t*>(smem + C::kT1);
+    uint32_t* sw = smem + C::kT1 + C::kT2 / 2;
+    uint32_t* sg = sw + C::kWordsPad;                    // gap words: sg[j] = gaps[s0/8 - 1 + j]
+    uint8_t* stage = reinterpret_cast<uint8_t*>(sg + C::kGapStage);
+    uint8_t* compact = stage + C::kStageBytes;
     __shared__ uint32_t warp_tot[C::kWarps];
-    __shared__ uint64_t s_tile;
+    __shared__ uint64_t s_tile[2];
     __shared__ uint64_t s_O;
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < C::kT1; i += kDecThreads) t1[i] = widen_entry(tab.t1[i]);
-    for (int i = tid; i < C::kT2; i += kDecThreads) t2[i] = widen_entry(tab.t2[i]);
-    for (int i = tid; i < C::kCompact; i += kDecThreads) compact[i] = 0;
+    for (int i = tid; i < C::kT2; i += kDecThreads) t2[i] = tab.t2[i];
     const uint64_t stream_bits = a.words * 32;
 
-    for (;;) {
-        if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
-        __syncthreads();
-        const uint64_t tile = s_tile;
-        if (tile >= a.ntiles) break;
-        const uint64_t s0 = tile * kDecSegs;
-        for (uint32_t i = tid; i < (uint32_t)C::kWords; i += kDecThreads) {
-            const uint64_t w = 4 * s0 + i;
-            sw[pidx(i)] = w < a.words ? ld_stream_u32(a.bits + w) : 0u;
-        }
-        __syncthreads();
+    // Loads of one tile's bitstream words and gap words into registers
+    // (issued a tile ahead) and their store into shared memory.
+#define HGAP_PREFETCH(T)                                                                      \
+    do {                                                                                      \
+        const uint64_t ps0 = (T) * kDecSegs;                                                  \
+        _Pragma("unroll") for (int j = 0; j < C::kWordsPer; ++j) {                            \
+            const uint32_t i = tid + j * kDecThreads;                                         \
+            const uint64_t w = 4 * ps0 + i;                                                   \
+            pre[j] = ((T) < a.ntiles && i < (uint32_t)C::kWords && w < a.words)               \
+                         ? ld_stream_u32(a.bits + w) : 0u;                                    \
+        }                                                                                     \
+        const int64_t g = (int64_t)(ps0 / 8) - 1 + (int64_t)tid;                              \
+        pre_gap = ((T) < a.ntiles && tid < (uint32_t)C::kGapStage && g >= 0 &&                \
+                   (uint64_t)g < a.gap_words) ? __ldg(a.gaps + g) : 0u;                       \
+    } while (0)
+#define HGAP_COMMIT()                                                                         \
+    do {                                                                                      \
+        _Pragma("unroll") for (int j = 0; j < C::kWordsPer; ++j) {                            \
+            const uint32_t i = tid + j * kDecThreads;                                         \
+            if (i < (uint32_t)C::kWords) sw[pidx(i)] = pre[j];                                \
+        }                                                                                     \
+        if (tid < (uint32_t)C::kGapStage) sg[tid] = pre_gap;                                  \
+    } while (0)
 
-        // ---- 1. decode segments tid and tid + 256 ---------------------------
-        uint32_t cnt[2];
+    uint32_t pre[C::kWordsPer];
+    uint32_t pre_gap = 0;
+    if (tid == 0) s_tile[0] = atomicAdd(a.counter, 1u);
+    __syncthreads();
+    uint64_t tile = s_tile[0];
+    HGAP_PREFETCH(tile);
+    HGAP_COMMIT();
+    uint32_t parity = 0;
+    // The tile decoded one iteration earlier: its symbols wait in `compact`
+    // (at tile-local offsets) until its output offset is resolved.
+    uint64_t prev = ~0ull;
+    uint32_t prev_ct = 0;
+
+    while (tile < a.ntiles || prev != ~0ull) {
+        __syncthreads();  // (1) words of `tile` staged; `compact` holds `prev`
+        const bool have = tile < a.ntiles;
+        const uint64_t s0 = tile * kDecSegs;
+        auto gap_of = [&](uint64_t k) -> uint32_t {  // k in [s0 - 1, s0 + 512)
+            const uint32_t j = (uint32_t)((k >> 3) - (s0 >> 3) + 1);
+            return (sg[j] >> (4 * (uint32_t)(k & 7))) & 0xfu;
+        };
+
+        // ---- 1. decode segments tid and tid + 256, one after the other ---------
+        uint32_t n[2] = {0, 0};
+        if (have) {
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint32_t col = tid + k * kDecThreads;
-            const uint64_t s = s0 + col;
-            uint32_t n = 0;
-            if (s < a.segments) {
-                const bool last = s + 1 == a.segments;
-                uint32_t pos = 128 * col + (s ? gap_entry(a.gaps, s - 1) : 0u);
-                uint32_t end = 128 * col + 128;
-                if (last && stream_bits - 128 * s0 < end) end = (uint32_t)(stream_bits - 128 * s0);
-                bool bad = false;
-                uint8_t* out = stage + col;
-                while (pos < end) {
-                    const uint32_t w = pos >> 5;
-                    const uint32_t x = __funnelshift_l(sw[pidx(w + 1)], sw[pidx(w)], pos);
-                    uint32_t e = t1[x >> (32 - kDecPrefix)];
-                    if (e & 0x80000000u) {  // longer than the prefix: level 2
-                        const uint32_t wd = (e >> 16) & 7u;
-                        e = t2[(e & 0xffffu) + ((x << kDecPrefix) >> (32 - wd))];
+            for (int k = 0; k < 2; ++k) {
+                const uint32_t col = tid + k * kDecThreads;
+                const uint64_t s = s0 + col;
+                uint32_t cnt = 0;
+                if (s < a.segments) {
+                    const bool last = s + 1 == a.segments;
+                    uint32_t pos = 128 * col + (s ? gap_of(s - 1) : 0u);
+                    uint32_t end = 128 * col + 128;
+                    if (last && stream_bits - 128 * s0 < end) end = (uint32_t)(stream_bits - 128 * s0);
+                    bool bad = false;
+                    uint8_t* out = stage + col;
+                    while (pos < end) {
+                        const uint32_t e = lookup(sw, t1, t2, pos);
+                        if ((e & 0x40000000u) || cnt >= (uint32_t)C::kMaxSym) {
+                            bad = !last;  // zero padding after the final codeword may not decode
+                            break;
+                        }
+                        *out = (uint8_t)e;
+                        out += C::kPitch;
+                        ++cnt;
+                        pos += (e >> 8) & 31u;
                     }
-                    if ((e & 0x40000000u) || n >= (uint32_t)C::kMaxSym) {
-                        bad = !last;  // zero padding after the final codeword may not decode
-                        break;
-                    }
-                    pos += (e >> 8) & 31u;
-                    *out = (uint8_t)e;
-                    out += kDecSegs;
-                    ++n;
+                    if (!last && !bad && pos != 128 * col + 128 + gap_of(s)) bad = true;
+                    if (bad) atomicOr(a.status, kDevCorrupt);
                 }
-                if (!last && !bad && pos != 128 * col + 128 + gap_entry(a.gaps, s)) bad = true;
-                if (bad) atomicOr(a.status, kDevCorrupt);
+                n[k] = cnt;
             }
-            cnt[k] = n;
         }
 
         // ---- 2. scan of the 512 counts (segments 0..255 are k = 0, 256..511 k = 1)
-        const uint32_t i0 = warp_incl_scan(cnt[0], lane);
-        const uint32_t i1 = warp_incl_scan(cnt[1], lane);
+        const uint32_t i0 = warp_incl_scan(n[0], lane);
+        const uint32_t i1 = warp_incl_scan(n[1], lane);
         if (lane == 31) warp_tot[warp] = i0 | (i1 << 16);  // a warp's 32 segments: < 2^13 symbols
-        __syncthreads();
+        if (tid == 0 && have) s_tile[parity ^ 1] = atomicAdd(a.counter, 1u);
+        __syncthreads();  // (2) decode done; next tile id known
+        const uint64_t next = have ? s_tile[parity ^ 1] : ~0ull;
         uint32_t wt = lane < (uint32_t)C::kWarps ? warp_tot[lane] : 0u;
-        uint32_t w0 = wt & 0xffffu, w1 = wt >> 16;
-        w0 = warp_incl_scan(w0, lane);
-        w1 = warp_incl_scan(w1, lane);
+        uint32_t w0 = warp_incl_scan(wt & 0xffffu, lane), w1 = warp_incl_scan(wt >> 16, lane);
         const uint32_t total0 = __shfl_sync(kFull, w0, C::kWarps - 1);
         const uint32_t total1 = __shfl_sync(kFull, w1, C::kWarps - 1);
         const uint32_t before0 = warp ? __shfl_sync(kFull, w0, warp - 1) : 0u;
         const uint32_t before1 = warp ? __shfl_sync(kFull, w1, warp - 1) : 0u;
         const uint32_t Ct = total0 + total1;
-        const uint32_t excl0 = before0 + i0 - cnt[0];
-        const uint32_t excl1 = total0 + before1 + i1 - cnt[1];
-        if (warp == 0) {
-            const uint64_t O = lookback_warp_wide<kDecLookK>(a.lookback, tile, Ct, a.status, lane);
+        const uint32_t excl[2] = {before0 + i0 - n[0], total0 + before1 + i1 - n[1]};
+        if (tid == 0 && have) lookback_publish(a.lookback, tile, Ct);
+        if (next < a.ntiles) HGAP_PREFETCH(next);  // in flight while `prev` is resolved and written
+        if (prev != ~0ull && warp == 0) {
+            const uint64_t O = lookback_resolve<kDecLookK>(a.lookback, prev, prev_ct, a.status, lane);
             if (lane == 0) s_O = O;
         }
-        __syncthreads();
-        const uint64_t O = s_O;
-        if (tid == 0 && tile + 1 == a.ntiles && O + Ct < a.n) atomicOr(a.status, kDevSize);
+        __syncthreads();  // (3) prev's output offset known
 
-        // ---- 3. compact into the 16-byte-aligned output image, write out -----
-        const uint64_t vstart = a.out_lo + O;
-        const uint32_t base = (uint32_t)(vstart & 15);
-        uint8_t* cbytes = reinterpret_cast<uint8_t*>(compact);
+        // ---- 3. write out `prev`: 16-byte output chunk q takes compact bytes
+        //         [16q - vstart, 16q - vstart + 16), i.e. parts of two aligned groups
+        if (prev != ~0ull) {
+            const uint64_t O = s_O;
+            const uint32_t Cp = prev_ct;
+            if (tid == 0 && prev + 1 == a.ntiles && O + Cp < a.n) atomicOr(a.status, kDevSize);
+            if (O < a.n) {
+                const uint64_t vstart = a.out_lo + O;
+                const uint64_t vend = a.out_lo + (O + Cp < a.n ? O + Cp : a.n);
+                const uint32_t base = (uint32_t)(vstart & 15);  // compact byte 0 sits at chunk offset base
+                const uint64_t q0 = vstart >> 4, q1 = (vend + 15) >> 4;
+                const uint32_t nq = (uint32_t)(q1 - q0);
+                for (uint32_t i0q = warp * 32; i0q < nq; i0q += kDecThreads) {
+                    const uint32_t lq = i0q + lane;  // chunk index within the tile
+                    // aligned compact group lq covers chunk lq's bytes [base, 16) and chunk lq+1's [0, base)
+                    uint4 g = make_uint4(0, 0, 0, 0);
+                    if (lq < nq) g = *reinterpret_cast<const uint4*>(compact + 16 * lq);
+                    uint4 p;  // group lq - 1
+                    p.x = __shfl_up_sync(kFull, g.x, 1);
+                    p.y = __shfl_up_sync(kFull, g.y, 1);
+                    p.z = __shfl_up_sync(kFull, g.z, 1);
+                    p.w = __shfl_up_sync(kFull, g.w, 1);
+                    if (lane == 0 && lq > 0) p = *reinterpret_cast<const uint4*>(compact + 16 * (lq - 1));
+                    if (lq >= nq) continue;
+                    // output byte b = byte 16 - base + b of the 32-byte pair (p, g): output word i
+                    // joins words k and k+1 of (p.x..p.w, g.x..g.w), k = 3 - base/4 + i
+                    const uint32_t sh = 8 * (base & 3);
+                    auto comb = [sh](uint32_t lo, uint32_t hi) { return sh ? __funnelshift_r(lo, hi, 32 - sh) : hi; };
+                    uint32_t o[4];
+                    switch (base >> 2) {  // uniform over the tile
+                        case 0: o[0] = comb(p.w, g.x); o[1] = comb(g.x, g.y); o[2] = comb(g.y, g.z); o[3] = comb(g.z, g.w); break;
+                        case 1: o[0] = comb(p.z, p.w); o[1] = comb(p.w, g.x); o[2] = comb(g.x, g.y); o[3] = comb(g.y, g.z); break;
+                        case 2: o[0] = comb(p.y, p.z); o[1] = comb(p.z, p.w); o[2] = comb(p.w, g.x); o[3] = comb(g.x, g.y); break;
+                        default: o[0] = comb(p.x, p.y); o[1] = comb(p.y, p.z); o[2] = comb(p.z, p.w); o[3] = comb(p.w, g.x); break;
+                    }
+                    const uint64_t c0 = (q0 + lq) << 4;
+                    if (c0 >= vstart && c0 + 16 <= vend) {
+                        *reinterpret_cast<uint4*>(a.out_aligned + c0) = make_uint4(o[0], o[1], o[2], o[3]);
+                    } else {
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint8_t* src = stage + tid + k * kDecThreads;
-            uint8_t* dst = cbytes + base + (k ? excl1 : excl0);
-            for (uint32_t j = 0; j < cnt[k]; ++j) dst[j] = src[j * kDecSegs];
-        }
-        __syncthreads();
-        if (O < a.n) {
-            const uint64_t stop = (O + Ct < a.n ? O + Ct : a.n);
-            const uint64_t vend = a.out_lo + stop;
-            const uint64_t q0 = vstart >> 4;
-            const uint64_t q1 = (vend + 15) >> 4;
-            for (uint64_t q = q0 + tid; q < q1; q += kDecThreads) {
-                const uint32_t lq = (uint32_t)(q - q0);
-                const uint64_t c0 = q << 4;
-                if (c0 >= vstart && c0 + 16 <= vend) {
-                    const uint4 v = reinterpret_cast<const uint4*>(compact)[lq];
-                    *reinterpret_cast<uint4*>(a.out_aligned + c0) = v;
-                } else {
-                    const uint8_t* cb = cbytes + 16 * lq;
-                    for (uint32_t b = 0; b < 16; ++b) {
-                        const uint64_t vb = c0 + b;
-                        if (vb >= vstart && vb < vend) a.out_aligned[vb] = cb[b];
+                        for (uint32_t b = 0; b < 16; ++b) {
+                            const uint64_t vb = c0 + b;
+                            if (vb >= vstart && vb < vend) a.out_aligned[vb] = (uint8_t)(o[b >> 2] >> (8 * (b & 3)));
+                        }
                     }
                 }
             }
         }
-        __syncthreads();
+        __syncthreads();  // (4) `compact` free again
+
+        // ---- 4. compact this tile at tile-local offsets (alignment applied on write-out)
+        if (have) {
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const uint8_t* src = stage + tid + k * kDecThreads;
+                uint8_t* dst = compact + excl[k];
+                for (uint32_t j = 0; j < n[k]; ++j) dst[j] = src[j * C::kPitch];
+            }
+        }
+        if (next < a.ntiles) HGAP_COMMIT();  // sw/sg are no longer read for this tile
+        prev = have ? tile : ~0ull;
+        prev_ct = Ct;
+        tile = have ? next : ~0ull;
+        parity ^= 1;
     }
+#undef HGAP_PREFETCH
+#undef HGAP_COMMIT
 }
 
 uint64_t decode_tiles(uint64_t segments) { return (segments + kDecSegs - 1) / kDecSegs; }

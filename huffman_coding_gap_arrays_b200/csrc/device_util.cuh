@@ -114,18 +114,24 @@ __device__ __forceinline__ uint64_t lookback_warp(uint64_t* rec, uint64_t tile, 
 }
 
 // The same look-back with a window of 32*K predecessors per round trip: lane
-// l inspects tiles top-K*l ... top-K*l-K+1 (nearest first).  The inclusive-
-// prefix frontier can advance only one window per L2 round trip, so the window
-// must exceed (tiles started per round trip); at the decoder's tile rate on a
-// B200 a 32-record window would cap the whole kernel.
+// l holds tiles top-K*l ... top-K*l-K+1 (nearest first, window position
+// K*l + j).  The inclusive-prefix frontier advances at most one window per L2
+// round trip, so the window must exceed the tiles started per round trip.
+// Only the records between the tile and the nearest inclusive prefix matter:
+// the window is loaded without blocking, and the warp waits only while an
+// unpublished record lies in front of the nearest inclusive prefix (on that
+// one record, bounded), then reloads.
+// Publishing the aggregate and resolving the prefix are separate steps, so a
+// CTA can publish a tile's aggregate, decode its next tile, and resolve the
+// first tile afterwards, when its predecessors have long been published.
+__device__ __forceinline__ void lookback_publish(uint64_t* rec, uint64_t tile, uint64_t agg) {
+    st_relaxed_u64(rec + tile, (tile == 0 ? kFlagP : kFlagA) | (agg & kValueMask));
+}
+
 template <int K>
-__device__ __forceinline__ uint64_t lookback_warp_wide(uint64_t* rec, uint64_t tile, uint64_t agg,
-                                                       uint32_t* status, uint32_t lane) {
-    if (tile == 0) {
-        if (lane == 0) st_relaxed_u64(rec, kFlagP | agg);
-        return 0;
-    }
-    if (lane == 0) st_relaxed_u64(rec + tile, kFlagA | agg);
+__device__ __forceinline__ uint64_t lookback_resolve(uint64_t* rec, uint64_t tile, uint64_t agg,
+                                                     uint32_t* status, uint32_t lane) {
+    if (tile == 0) return 0;
     uint64_t excl = 0;
     int64_t top = (int64_t)tile - 1;
     for (;;) {
@@ -135,25 +141,33 @@ __device__ __forceinline__ uint64_t lookback_warp_wide(uint64_t* rec, uint64_t t
             const int64_t i = top - (int64_t)(K * lane + j);
             v[j] = i >= 0 ? ld_relaxed_u64(rec + i) : kFlagP;
         }
+        int first_p = K, first_z = K;  // nearest inclusive prefix / unpublished record of this lane
 #pragma unroll
-        for (int j = 0; j < K; ++j) {
-            const int64_t i = top - (int64_t)(K * lane + j);
-            if (v[j] == 0) v[j] = wait_nonzero(rec + i, status, kFlagP);
+        for (int j = K - 1; j >= 0; --j) {
+            if (v[j] & kFlagP) first_p = j;
+            if (v[j] == 0) first_z = j;
         }
-        int first = K;  // nearest record of this lane with an inclusive prefix
-#pragma unroll
-        for (int j = K - 1; j >= 0; --j)
-            if (v[j] & kFlagP) first = j;
-        const uint32_t pmask = __ballot_sync(kFull, first < K);
-        const int fl = pmask ? __ffs(pmask) - 1 : 32;
+        const uint32_t pmask = __ballot_sync(kFull, first_p < K);
+        const uint32_t zmask = __ballot_sync(kFull, first_z < K);
+        const int lp = pmask ? __ffs(pmask) - 1 : 32;
+        const int lz = zmask ? __ffs(zmask) - 1 : 32;
+        const int gp = lp < 32 ? K * lp + __shfl_sync(kFull, first_p, lp) : 32 * K;
+        const int gz = lz < 32 ? K * lz + __shfl_sync(kFull, first_z, lz) : 32 * K;
+        if (gz < gp) {  // an unpublished record in front of the nearest inclusive prefix
+            if ((int)lane == lz) {
+                const int64_t i = top - (int64_t)gz;
+                wait_nonzero(rec + i, status, kFlagP);
+            }
+            __syncwarp();
+            if (ld_relaxed_u32(status) & kDevTimeout) return excl;  // gave up: the status says so
+            continue;  // reload the same window
+        }
         uint64_t sum = 0;
 #pragma unroll
-        for (int j = 0; j < K; ++j) {
-            const bool take = (int)lane < fl || ((int)lane == fl && j <= first);
-            if (take) sum += v[j] & kValueMask;
-        }
+        for (int j = 0; j < K; ++j)
+            if ((int)(K * lane + j) <= gp) sum += v[j] & kValueMask;
         excl += warp_sum_u64(sum);
-        if (pmask) break;
+        if (gp < 32 * K) break;
         top -= 32 * K;
     }
     if (lane == 0) st_relaxed_u64(rec + tile, kFlagP | ((excl + agg) & kValueMask));

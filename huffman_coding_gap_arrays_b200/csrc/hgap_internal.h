@@ -119,6 +119,7 @@ struct DecArgs {
     uint64_t words;
     const uint32_t* gaps;
     uint64_t segments;
+    uint64_t gap_words;
     uint8_t* out_aligned;  // output rounded down to 16 bytes
     uint64_t out_lo;       // out & 15
     uint64_t n;
