@@ -197,9 +197,13 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (cudaMemsetAsync(ws, 0, need, st) != cudaSuccess) return HGAP_ERR_CUDA;
     uint32_t min_len = hgap::kMaxLen;
-    for (uint32_t i = 0; i < book.symbol_count; ++i)
+    uint64_t kraft = 0;  // units of 2^-16; a complete book (sum 1) has no invalid table entry
+    for (uint32_t i = 0; i < book.symbol_count; ++i) {
         if (book.symbols[i].length < min_len) min_len = book.symbols[i].length;
-    return cuda_status(hgap::launch_decode(a, t, min_len, stream));
+        kraft += 1ull << (hgap::kMaxLen - book.symbols[i].length);
+    }
+    const bool complete = kraft == (1ull << hgap::kMaxLen);
+    return cuda_status(hgap::launch_decode(a, t, min_len, complete, stream));
 }
 
 hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream) {

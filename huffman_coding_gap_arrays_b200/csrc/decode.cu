@@ -49,12 +49,12 @@ struct DecCfg {
                   kStageBytes % 16 == 0, "16-byte aligned areas");
 };
 
-// Level-1 table entry in shared memory (u32): direct = len << 8 | symbol;
+// Table entry in shared memory (u32): direct = len << 24 | symbol;
 // pointer = bit 31 | extra width << 16 | level-2 offset; invalid = bit 30.
 __device__ __forceinline__ uint32_t widen_entry(uint32_t e) {
     if (e & 0x8000u) return 0x80000000u | (((e >> 12) & 7u) << 16) | (e & 0xfffu);
     if (e & kDecInvalid) return 0x40000000u;
-    return ((((e >> 8) & 15u) + 1u) << 8) | (e & 0xffu);
+    return ((((e >> 8) & 15u) + 1u) << 24) | (e & 0xffu);
 }
 
 __device__ __forceinline__ uint32_t pidx(uint32_t w) { return w + (w >> 3); }
@@ -73,7 +73,9 @@ __device__ __forceinline__ uint32_t lookup(const uint32_t* sw, const uint32_t* t
     return e;
 }
 
-template <int R>
+// COMPLETE: the book's Kraft sum is 1 (every package-merge book with two or
+// more symbols), so no table entry is invalid and the decode loop skips that test.
+template <int R, bool COMPLETE>
 __global__ void __launch_bounds__(kDecThreads, 3)
     decode_kernel(const DecArgs a, const __grid_constant__ DecTable tab) {
     using C = DecCfg<R>;
@@ -154,17 +156,19 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                     if (last && stream_bits - 128 * s0 < end) end = (uint32_t)(stream_bits - 128 * s0);
                     bool bad = false;
                     uint8_t* out = stage + col;
+                    // every codeword is at least the book's shortest length, so a
+                    // segment yields at most kMaxSym symbols: no count test needed
                     while (pos < end) {
                         const uint32_t e = lookup(sw, t1, t2, pos);
-                        if ((e & 0x40000000u) || cnt >= (uint32_t)C::kMaxSym) {
+                        if (!COMPLETE && (e & 0x40000000u)) {
                             bad = !last;  // zero padding after the final codeword may not decode
                             break;
                         }
                         *out = (uint8_t)e;
                         out += C::kPitch;
-                        ++cnt;
-                        pos += (e >> 8) & 31u;
+                        pos += e >> 24;
                     }
+                    cnt = (uint32_t)(out - (stage + col)) / C::kPitch;
                     if (!last && !bad && pos != 128 * col + 128 + gap_of(s)) bad = true;
                     if (bad) atomicOr(a.status, kDevCorrupt);
                 }
@@ -266,35 +270,40 @@ __global__ void __launch_bounds__(kDecThreads, 3)
 
 uint64_t decode_tiles(uint64_t segments) { return (segments + kDecSegs - 1) / kDecSegs; }
 
-template <int R>
+template <int R, bool COMPLETE>
 static int launch_decode_r(const DecArgs& a, const DecTable& t, cudaStream_t st) {
     using C = DecCfg<R>;
+    auto kern = decode_kernel<R, COMPLETE>;
     static int sms = 0, per_sm = 0;
     if (sms == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaError_t e = cudaFuncSetAttribute(decode_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)C::kSmem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::kSmem);
         if (e != cudaSuccess) return e;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, decode_kernel<R>, kDecThreads, C::kSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kDecThreads, C::kSmem);
         if (per_sm < 1) per_sm = 1;
     }
     const uint64_t cap = (uint64_t)sms * per_sm;
     const unsigned grid = (unsigned)(a.ntiles < cap ? a.ntiles : cap);
-    decode_kernel<R><<<grid, kDecThreads, C::kSmem, st>>>(a, t);
+    kern<<<grid, kDecThreads, C::kSmem, st>>>(a, t);
     return cudaGetLastError();
+}
+
+template <bool COMPLETE>
+static int launch_decode_c(const DecArgs& a, const DecTable& t, uint32_t max_sym, cudaStream_t st) {
+    if (max_sym <= 32) return launch_decode_r<8, COMPLETE>(a, t, st);
+    if (max_sym <= 44) return launch_decode_r<11, COMPLETE>(a, t, st);
+    if (max_sym <= 64) return launch_decode_r<16, COMPLETE>(a, t, st);
+    return launch_decode_r<32, COMPLETE>(a, t, st);
 }
 
 // min_len: shortest code length of the book.  A segment holds at most
 // ceil(128 / min_len) codeword starts; the stage is sized for that.
-int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, void* stream) {
+int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const uint32_t max_sym = (128 + min_len - 1) / (min_len ? min_len : 1);
-    if (max_sym <= 32) return launch_decode_r<8>(a, t, st);
-    if (max_sym <= 44) return launch_decode_r<11>(a, t, st);
-    if (max_sym <= 64) return launch_decode_r<16>(a, t, st);
-    return launch_decode_r<32>(a, t, st);
+    return complete ? launch_decode_c<true>(a, t, max_sym, st) : launch_decode_c<false>(a, t, max_sym, st);
 }
 
 }  // namespace hgap

@@ -134,7 +134,7 @@ struct DecArgs {
 int launch_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, void* stream);
 int launch_encode(const EncArgs& a, const EncTable& t, void* stream);
 int launch_hist_st(const HistStArgs& a, void* stream);
-int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, void* stream);
+int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, void* stream);
 uint64_t decode_tiles(uint64_t segments);
 
 // ------------------------------------------------------------- host helpers -
