@@ -7,25 +7,33 @@
 // id by persistent CTAs of 512 threads.  Its bit count is one dot product of
 // its histogram (recorded by hist_st_kernel in the same pass that builds the
 // global histogram) with the code lengths, so a single bounded look-back over
-// super-tiles gives its first output bit G right away; no per-chunk look-back
-// and no waiting on neighbours afterwards.  The CTA then streams its chunks in
-// order, carrying the running bit offset:
-//   * 16-byte load per thread (next chunk prefetched while this one packs);
+// super-tiles gives its first output bit G; no per-chunk look-back and no
+// waiting on neighbours afterwards.  A CTA claims its next super-tile one
+// ahead and publishes that one's bit count at once, so no look-back ever
+// waits on a claimed super-tile, and the input stream never drains between
+// super-tiles.
+//
+// Input: chunks are staged in a ring of kRing shared-memory buffers by 1-D
+// bulk copies (TMA engine, completion on an mbarrier), issued by one thread
+// kRing chunks ahead of the one being encoded: 48 KiB per SM in flight, which
+// a one-load-per-thread register prefetch cannot reach.
+//
+// Per chunk:
 //   * lookups in a 32-way lane-replicated codeword table ([byte][lane]: each
 //     lane reads its own bank, never a conflict);
 //   * one block scan of per-thread bit counts (warp scan + 16 warp totals);
-//   * packing with a 64-bit accumulator into a shared image of the output
-//     words, indexed from the segment-aligned word below the chunk's first
-//     bit, so the image's 16-byte groups are the output's 16-byte groups;
-//     word emission is predicated (no divergent branch); the one word a
-//     thread shares with each neighbour is OR-ed in with a shared atomic;
+//   * packing two codes at a time (<= 32 bits) into a shared image of the
+//     output words, indexed from the segment-aligned word below the chunk's
+//     first bit, so the image's 16-byte groups are the output's 16-byte
+//     groups; the word a thread shares with a neighbour is OR-ed in with a
+//     shared atomic;
 //   * a gap entry falls out of word completion: the code completing global
 //     word w with w % 4 == 3 ends segment w/4 and its spill into the next
 //     word is that segment's entry (encoder/src/encoder.cu:307-312); each
 //     segment has exactly one such code, so entries are plain byte stores;
-//   * complete words go out with 16-byte coalesced stores; the partial last
-//     word and gap word are carried to the next chunk (double-buffered image,
-//     two barriers per chunk).
+//   * complete words go out with 16-byte coalesced stores, and each group of
+//     the image is cleared right after it is read; the partial last word and
+//     gap word are carried to the next chunk.  Two barriers per chunk.
 // The super-tile's first partial word and gap word also hold bits of the
 // previous super-tile; one warp rebuilds those by re-encoding at most 1023
 // bits backwards from G (the predecessor's last bytes), so neighbouring
@@ -41,40 +49,90 @@ constexpr int kEncThreads = 512;
 constexpr int kEncBpt = 16;
 constexpr int kEncWarps = kEncThreads / 32;
 static_assert(kEncThreads * kEncBpt == kEncChunkBytes, "chunk = threads x bytes per thread");
-constexpr int kStgWords = kEncChunkBytes * 16 / 32 + 16;    // <= 16 bits per byte, + carry/alignment
-constexpr int kGapWords = kEncChunkBytes * 16 / 1024 + 8;
+constexpr int kRing = 3;                                  // input chunks staged ahead
+constexpr int kImgWords = kEncChunkBytes * 16 / 32 + 16;  // <= 16 bits per byte, + carry/alignment
 constexpr int kLutWords = 256 * 32;
-// two lane-replicated tables (left-aligned codes, lengths), two output images,
-// two gap-word carries, one spill byte per image word
-constexpr size_t kEncSmem = (size_t)(2 * kLutWords + 2 * kStgWords + 2 * kGapWords) * 4 + kStgWords;
+// two lane-replicated tables (left-aligned codes, lengths), the input ring,
+// the output image and one spill byte per image word
+constexpr size_t kEncSmem =
+    (size_t)2 * kLutWords * 4 + (size_t)kRing * kEncChunkBytes + (size_t)kImgWords * 4 + kImgWords;
 
 struct EncShared {
+    uint64_t mbar[kRing];       // one per ring buffer: its bulk copy landed
+    uint64_t G;                 // first output bit of the current super-tile
+    uint64_t cur;               // super-tile being encoded
+    uint64_t agg_cur;           // its bit count
     uint32_t warp_tot[kEncWarps];
-    uint64_t red[kEncWarps];
-    uint64_t st;
-    uint64_t G;
+    uint32_t carry;             // partial output word carried into the next chunk
+    uint32_t gcarry[2];         // partial gap word carried, by chunk parity
     uint32_t abort;
 };
 
-__device__ __forceinline__ uint64_t block_sum_u64(uint64_t v, EncShared& sh, uint32_t lane,
-                                                  uint32_t warp) {
-    v = warp_sum_u64(v);
-    if (lane == 0) sh.red[warp] = v;
-    __syncthreads();
-    uint64_t t = 0;
+// Warp 0: claims a super-tile and publishes its bit count right away, so that
+// no later super-tile's look-back waits on it.
+__device__ __forceinline__ void claim_super_tile(const EncArgs& a, const uint32_t* lutl, uint32_t lane,
+                                                 uint64_t& st, uint64_t& agg) {
+    uint32_t s = 0;
+    if (lane == 0) s = atomicAdd(a.counter, 1u);
+    st = __shfl_sync(kFull, s, 0);
+    agg = 0;
+    if (st < a.nst) {
+        uint64_t part = 0;
 #pragma unroll
-    for (int i = 0; i < kEncWarps; ++i) t += sh.red[i];
-    return t;
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t b = lane + 32 * j;
+            part += (uint64_t)a.st_hist[st * 256 + b] * (lutl[b << 5] & 31u);
+        }
+        agg = warp_sum_u64(part);
+        if (lane == 0) lookback_publish(a.st_rec, st, agg);
+    }
 }
+
+__device__ __forceinline__ uint32_t st_chunks(const EncArgs& a, uint64_t st) {
+    const uint64_t v0 = st * (uint64_t)a.st_bytes;
+    const uint64_t v1 = (v0 + a.st_bytes < a.hi) ? v0 + a.st_bytes : a.hi;
+    return (uint32_t)((v1 - v0 + kEncChunkBytes - 1) / kEncChunkBytes);
+}
+
+// Thread 0's bulk-copy producer.  Copies go out in the order the CTA encodes
+// chunks: the rest of the current super-tile, then the claimed next one; at
+// most kRing beyond the last chunk whose buffer is free again.
+struct Producer {
+    uint32_t issued = 0;  // copies issued so far (chunk sequence number)
+    uint64_t pst = ~0ull; // super-tile of the next copy
+    uint32_t pc = 0;      // its chunk index
+
+    __device__ __forceinline__ void run(const EncArgs& a, uint8_t* ring, EncShared& sh, uint32_t freed,
+                                        uint64_t cur, uint64_t nxt) {
+        while (issued < freed + kRing) {
+            if (pst >= a.nst) break;
+            if (pc >= st_chunks(a, pst)) {
+                if (pst == cur && nxt < a.nst) {
+                    pst = nxt;
+                    pc = 0;
+                    continue;
+                }
+                break;  // wait for the next claim
+            }
+            const uint64_t v = pst * (uint64_t)a.st_bytes + (uint64_t)pc * kEncChunkBytes;
+            const uint64_t rem = ((a.hi + 15) & ~15ull) - v;  // through the end of the last 16-byte group
+            const uint32_t bytes = rem >= (uint64_t)kEncChunkBytes ? (uint32_t)kEncChunkBytes : (uint32_t)rem;
+            const uint32_t s = issued % kRing;
+            bulk_load(ring + (size_t)s * kEncChunkBytes, a.in_aligned + v, bytes, &sh.mbar[s]);
+            ++issued;
+            ++pc;
+        }
+    }
+};
 
 __global__ void __launch_bounds__(kEncThreads, 2)
     encode_kernel(const EncArgs a, const __grid_constant__ EncTable tab) {
     extern __shared__ __align__(16) uint32_t smem[];
-    uint32_t* lutc = smem;                         // [byte][lane]: code << (32 - len)
-    uint32_t* lutl = smem + kLutWords;             // [byte][lane]: len (0x200 if absent)
-    uint32_t* stg0 = smem + 2 * kLutWords;         // two output images, ping-pong per chunk
-    uint32_t* gst0 = stg0 + 2 * kStgWords;         // two gap-word carries
-    uint8_t* spills = reinterpret_cast<uint8_t*>(gst0 + 2 * kGapWords);  // per image word
+    uint32_t* lutc = smem;                // [byte][lane]: code << (32 - len)
+    uint32_t* lutl = smem + kLutWords;    // [byte][lane]: len (0x200 if absent)
+    uint8_t* ring = reinterpret_cast<uint8_t*>(smem + 2 * kLutWords);  // kRing input chunks
+    uint32_t* img = reinterpret_cast<uint32_t*>(ring + (size_t)kRing * kEncChunkBytes);
+    uint8_t* spills = reinterpret_cast<uint8_t*>(img + kImgWords);     // per image word
     __shared__ EncShared sh;
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -84,97 +142,100 @@ __global__ void __launch_bounds__(kEncThreads, 2)
         lutc[i] = l ? (e & 0xffffu) << (32 - l) : 0u;
         lutl[i] = (e == kEncAbsent) ? 0x200u : l;
     }
+    for (int i = tid; i < kImgWords; i += kEncThreads) img[i] = 0;
     if (tid == 0) {
         // the histograms in the workspace must come from this very input
         sh.abort = (a.tag[0] != a.hi - a.lo ||
                     a.tag[1] != reinterpret_cast<uint64_t>(a.in_aligned) + a.lo);
         if (sh.abort) atomicOr(a.status, kDevPlan);
+        for (int s = 0; s < kRing; ++s) mbar_init(&sh.mbar[s], 1);
+        mbar_init_fence();
     }
     __syncthreads();
     if (sh.abort) return;
     const bool vec_ok = a.bits_aligned16 != 0;
 
-    for (;;) {
-        __syncthreads();  // the previous super-tile is finished, its tail words included
-        for (int i = tid; i < 2 * (kStgWords + kGapWords); i += kEncThreads) stg0[i] = 0;
-        if (tid == 0) sh.st = atomicAdd(a.counter, 1u);
-        __syncthreads();
-        const uint64_t st = sh.st;
-        if (st >= a.nst) break;
+    Producer prod;                  // used by thread 0 only
+    uint64_t cur = 0, nxt = ~0ull;  // warp 0: super-tile being encoded, the one claimed next
+    uint64_t agg_cur = 0, agg_nxt = 0;
+    if (warp == 0) {
+        claim_super_tile(a, lutl, lane, cur, agg_cur);
+        if (cur < a.nst) claim_super_tile(a, lutl, lane, nxt, agg_nxt);
+        if (lane == 0) {
+            prod.pst = cur;
+            prod.run(a, ring, sh, 0, cur, nxt);
+        }
+    }
+    uint32_t cons = 0;  // chunks consumed so far (the ring's sequence number)
 
-        // ---- super-tile bit count, look-back, bits before G -----------------
-        uint64_t part = 0;
-        if (tid < 256) part = (uint64_t)a.st_hist[st * 256 + tid] * (lutl[tid << 5] & 31u);
-        const uint64_t agg = block_sum_u64(part, sh, lane, warp);
+    for (;;) {
+        // ---- warp 0: G of the current super-tile, bits before G -------------
         if (warp == 0) {
-            const uint64_t G = lookback_warp(a.st_rec, st, agg, a.status, lane);
-            if (lane == 0) sh.G = G;
-            const uint32_t r = (uint32_t)(G & 31);
-            const uint32_t nibs = (uint32_t)((G >> 7) & 7);
-            if (G > 0 && (r != 0 || nibs != 0)) {
-                // walk the previous super-tile's codes backwards from G
-                const uint64_t wstart = G - r;
-                const uint64_t gs = (G >> 10) << 10;
-                // codes starting at or below `stop` can no longer reach the head word
-                // (bits >= wstart) nor cross a boundary >= gs + 128
-                uint64_t stop = r ? wstart : ~0ull;
-                if (nibs && gs + 127 < stop) stop = gs + 127;
-                uint32_t head = 0;
-                uint64_t end = G;
-                const uint64_t vfirst = st * (uint64_t)a.st_bytes;  // first byte of this super-tile
-                for (uint64_t base = 0;; base += 32) {
-                    const uint64_t v = vfirst - 1 - base - lane;    // may wrap below lo: no byte
-                    uint32_t c = 0, len = 0;
-                    if (vfirst >= base + lane + 1 && v >= a.lo) {
-                        const uint32_t byte = __ldg(a.in_aligned + v);
-                        c = lutc[(byte << 5) | lane];
-                        len = lutl[(byte << 5) | lane] & 31u;
-                    }
-                    const uint32_t incl = warp_incl_scan(len, lane);
-                    const uint64_t ce = end - (incl - len);          // this code's end bit
-                    const uint64_t cs = ce - len;                    // and start bit
-                    if (len) {
-                        if (r && ce > wstart)  // the code's right-aligned value, placed to end at ce
-                            head |= (uint32_t)(((uint64_t)(c >> (32 - len))) << (wstart + 32 - ce));
-                        const uint64_t b = (ce >> 7) << 7;           // last segment boundary <= end
-                        if (nibs && b > cs && b >= gs + 128) {
-                            const uint64_t k = (b >> 7) - 1;
-                            atomicOr(gst0, (uint32_t)(ce - b) << (4 * (uint32_t)(k & 7)));
+            uint64_t G = 0;
+            uint32_t head = 0, gcarry = 0;
+            if (cur < a.nst) {
+                G = lookback_resolve<4>(a.st_rec, cur, agg_cur, a.status, lane);
+                const uint32_t r = (uint32_t)(G & 31);
+                const uint32_t nibs = (uint32_t)((G >> 7) & 7);
+                if (G > 0 && (r != 0 || nibs != 0)) {
+                    // walk the previous super-tile's codes backwards from G
+                    const uint64_t wstart = G - r;
+                    const uint64_t gs = (G >> 10) << 10;
+                    // codes starting at or below `stop` can no longer reach the head
+                    // word (bits >= wstart) nor cross a boundary >= gs + 128
+                    uint64_t stop = r ? wstart : ~0ull;
+                    if (nibs && gs + 127 < stop) stop = gs + 127;
+                    uint64_t end = G;
+                    const uint64_t vfirst = cur * (uint64_t)a.st_bytes;  // first byte of this super-tile
+                    for (uint64_t base = 0;; base += 32) {
+                        const uint64_t v = vfirst - 1 - base - lane;     // may wrap below lo: no byte
+                        uint32_t c = 0, len = 0;
+                        if (vfirst >= base + lane + 1 && v >= a.lo) {
+                            const uint32_t byte = __ldg(a.in_aligned + v);
+                            c = lutc[(byte << 5) | lane];
+                            len = lutl[(byte << 5) | lane] & 31u;
                         }
+                        const uint32_t incl = warp_incl_scan(len, lane);
+                        const uint64_t ce = end - (incl - len);  // this code's end bit
+                        const uint64_t cs = ce - len;            // and start bit
+                        if (len) {
+                            if (r && ce > wstart)  // the code's right-aligned value, placed to end at ce
+                                head |= (uint32_t)(((uint64_t)(c >> (32 - len))) << (wstart + 32 - ce));
+                            const uint64_t b = (ce >> 7) << 7;   // last segment boundary <= end
+                            if (nibs && b > cs && b >= gs + 128)
+                                gcarry |= (uint32_t)(ce - b) << (4 * (uint32_t)(((b >> 7) - 1) & 7));
+                        }
+                        const uint32_t total = __shfl_sync(kFull, incl, 31);
+                        const uint64_t smin = end - total;  // start of the batch's last code
+                        end = smin;
+                        if (smin <= stop || total == 0) break;
                     }
-                    const uint32_t total = __shfl_sync(kFull, incl, 31);
-                    const uint64_t smin = end - total;               // start of the batch's last code
-                    end = smin;
-                    if (smin <= stop || total == 0) break;
+                    head = __reduce_or_sync(kFull, head);
+                    gcarry = __reduce_or_sync(kFull, gcarry);
                 }
-                head = __reduce_or_sync(kFull, head);
-                if (lane == 0 && r) stg0[(G >> 5) & 3] = head;
+            }
+            if (lane == 0) {
+                sh.cur = cur;
+                sh.agg_cur = agg_cur;
+                sh.G = G;
+                sh.carry = head;  // 0 unless G % 32 != 0
+                sh.gcarry[cons & 1] = gcarry;
             }
         }
         __syncthreads();
+        const uint64_t st = sh.cur;
+        if (st >= a.nst) break;
         uint64_t P = sh.G;
-        uint64_t P_st = P;
+        const uint64_t P_st = P;
 
-        // ---- stream the chunks ---------------------------------------------
+        // ---- stream the chunks ----------------------------------------------
         const uint64_t v_st = st * (uint64_t)a.st_bytes;
-        uint64_t v_end = v_st + a.st_bytes;
-        if (v_end > a.hi) v_end = a.hi;
-        const uint32_t nchunks = (uint32_t)((v_end - v_st + kEncChunkBytes - 1) / kEncChunkBytes);
-        auto load = [&](uint32_t c) -> uint4 {
-            const uint64_t v = v_st + (uint64_t)c * kEncChunkBytes + (uint64_t)tid * kEncBpt;
-            uint4 q = make_uint4(0, 0, 0, 0);
-            if (c < nchunks && v < a.hi && v + 16 > a.lo) q = ld_stream_v4(a.in_aligned + v);
-            return q;
-        };
-        uint4 q_next = load(0);
-        uint32_t prev_used = 0;  // image words touched by the previous chunk
-        for (uint32_t c = 0; c < nchunks; ++c) {
-            const uint4 q = q_next;
-            q_next = load(c + 1);
-            uint32_t* stg = stg0 + (c & 1) * kStgWords;
-            uint32_t* stg_next = stg0 + ((c + 1) & 1) * kStgWords;
-            uint32_t* gst = gst0 + (c & 1) * kGapWords;
-            uint32_t* gst_next = gst0 + ((c + 1) & 1) * kGapWords;
+        const uint32_t nchunks = st_chunks(a, st);
+        bool overflow = false;
+        for (uint32_t c = 0; c < nchunks; ++c, ++cons) {
+            const uint32_t stage = cons % kRing;
+            mbar_wait(&sh.mbar[stage], (cons / kRing) & 1, a.status, true);
+            const uint4 q = *reinterpret_cast<const uint4*>(ring + (size_t)stage * kEncChunkBytes + tid * 16);
 
             // lookups: left-aligned code and length per byte, bit count per thread
             const uint64_t v0 = v_st + (uint64_t)c * kEncChunkBytes + (uint64_t)tid * kEncBpt;
@@ -209,69 +270,80 @@ __global__ void __launch_bounds__(kEncThreads, 2)
             }
             const uint32_t incl = warp_incl_scan(nbits, lane);
             if (lane == 31) sh.warp_tot[warp] = incl;
-            __syncthreads();  // (1) warp totals visible; previous chunk fully written out
-            // the previous chunk's image is free again: clear it for the next chunk
-            for (uint32_t i = 4 * tid; i < prev_used; i += 4 * kEncThreads)
-                *reinterpret_cast<uint4*>(stg_next + i) = make_uint4(0, 0, 0, 0);
+            __syncthreads();  // (1) warp totals visible; this ring buffer read; previous chunk written out
+            if (tid == 0) {
+                // the word carried in (previous chunk's tail, or the rebuilt head word)
+                if (sh.carry) atomicOr(img + ((P >> 5) & 3), sh.carry);
+                fence_proxy_async_smem();
+                prod.run(a, ring, sh, cons + 1, cur, nxt);
+            }
             uint32_t wt = lane < (uint32_t)kEncWarps ? sh.warp_tot[lane] : 0u;
             wt = warp_incl_scan(wt, lane);
             const uint32_t L = __shfl_sync(kFull, wt, kEncWarps - 1);
             const uint32_t excl = incl - nbits + (warp ? __shfl_sync(kFull, wt, warp - 1) : 0u);
 
-            // pack two codes per step (<= 32 bits), at most one word per step
+            // pack two codes at a time (<= 32 bits): at most one word per pair
             const uint64_t sb = (P >> 5) & ~3ull;  // segment-aligned image base (global word)
             if (nbits) {
                 const uint32_t p = (uint32_t)(P - 32 * sb) + excl;  // bit offset within the image
                 uint32_t wi = p >> 5;
                 uint32_t nb = p & 31;
                 bool first_shared = nb != 0;  // first word also holds the left neighbour's bits
-                uint32_t cur = 0;
+                uint32_t cur_w = 0;
 #pragma unroll
                 for (int k = 0; k < kEncBpt; k += 2) {
                     const uint32_t l1 = ll[k];
                     const uint32_t c12 = cc[k] | (cc[k + 1] >> l1);
                     const uint32_t nbo = nb;
-                    cur |= c12 >> nb;
+                    cur_w |= c12 >> nb;
                     const uint32_t spill = __funnelshift_r(0u, c12, nb);
                     nb += l1 + ll[k + 1];
                     if (nb >= 32) {
-                        if (first_shared) atomicOr(stg + wi, cur);
-                        else stg[wi] = cur;
+                        if (first_shared) atomicOr(img + wi, cur_w);
+                        else img[wi] = cur_w;
                         first_shared = false;
                         // bits of the code crossing the word end that spill over
                         spills[wi] = (uint8_t)(nbo + l1 >= 32 ? nbo + l1 - 32 : nb - 32);
                         ++wi;
-                        cur = spill;
+                        cur_w = spill;
                         nb -= 32;
                     }
                 }
-                if (nb) atomicOr(stg + wi, cur);
+                if (nb) atomicOr(img + wi, cur_w);
             }
             __syncthreads();  // (2) image complete
 
-            // write out complete words [P>>5, E>>5) and gap words [P>>10, kn>>3)
+            // write out complete words [P>>5, E>>5), clearing the image behind;
+            // the group holding word E>>5 hands it on as the carry
             const uint64_t E = P + L;
             const uint32_t j0 = (uint32_t)((P >> 5) - sb);
             const uint32_t j1 = (uint32_t)((E >> 5) - sb);
-            bool overflow = false;
-            for (uint32_t g = tid; g < (j1 + 3) / 4; g += kEncThreads) {
+            for (uint32_t g = tid; g <= j1 / 4; g += kEncThreads) {
                 const uint32_t j = 4 * g;
+                const uint4 wv = *reinterpret_cast<const uint4*>(img + j);
                 const uint64_t w = sb + j;
                 if (vec_ok && j >= j0 && j + 4 <= j1 && w + 4 <= a.words) {
-                    *reinterpret_cast<uint4*>(a.bits + w) = *reinterpret_cast<const uint4*>(stg + j);
+                    *reinterpret_cast<uint4*>(a.bits + w) = wv;
                 } else {
+                    const uint32_t wa[4] = {wv.x, wv.y, wv.z, wv.w};
 #pragma unroll
                     for (uint32_t k = 0; k < 4; ++k) {
                         if (j + k < j0 || j + k >= j1) continue;
-                        if (w + k < a.words) a.bits[w + k] = stg[j + k];
+                        if (w + k < a.words) a.bits[w + k] = wa[k];
                         else overflow = true;
                     }
+                    if (j1 - j < 4) {
+                        const uint32_t t = j1 - j;
+                        sh.carry = (E & 31) ? (t == 0 ? wa[0] : t == 1 ? wa[1] : t == 2 ? wa[2] : wa[3]) : 0u;
+                    }
                 }
+                *reinterpret_cast<uint4*>(img + j) = make_uint4(0, 0, 0, 0);
             }
+            // gap words [P>>10, kn>>3); word kn>>3 is partial (or empty) and carried
             const uint64_t kb = P >> 7, kn = E >> 7;  // segments ending in this chunk: [kb, kn)
             const uint64_t gwb = P >> 10, gwe = kn >> 3;
             for (uint64_t g = gwb + tid; g <= gwe; g += kEncThreads) {
-                uint32_t v = (g == gwb) ? gst[0] : 0u;
+                uint32_t v = (g == gwb) ? sh.gcarry[cons & 1] : 0u;
                 const uint64_t k0 = (8 * g > kb) ? 8 * g : kb;
                 const uint64_t k1 = (8 * g + 8 < kn) ? 8 * g + 8 : kn;
                 for (uint64_t k = k0; k < k1; ++k)  // entry k = spill of global word 4k+3
@@ -280,27 +352,38 @@ __global__ void __launch_bounds__(kEncThreads, 2)
                     if (g < a.gap_words) a.gaps[g] = v;
                     else overflow = true;
                 } else {
-                    gst_next[0] = v;  // partial gap word carried to the next chunk
+                    sh.gcarry[(cons + 1) & 1] = v;
                 }
             }
-            if (tid == 0) stg_next[(E >> 5) & 3] = stg[j1];  // partial word carried
-            if (overflow) atomicOr(a.status, kDevSize);
-            prev_used = j1 + 2;
             P = E;
         }
-        __syncthreads();  // carries visible
+        if (overflow) atomicOr(a.status, kDevSize);
+        __syncthreads();  // carries visible; the image is clear again
+
         // ---- end of the super-tile ------------------------------------------
         if (tid == 0) {
-            if (P - P_st != agg) atomicOr(a.status, kDevPlan);  // histograms were not this input's
+            if (P - P_st != sh.agg_cur) atomicOr(a.status, kDevPlan);  // histograms were not this input's
             if (st + 1 == a.nst) {
-                const uint32_t* stg = stg0 + (nchunks & 1) * kStgWords;
-                const uint32_t* gst = gst0 + (nchunks & 1) * kGapWords;
-                if ((P & 31) && (P >> 5) < a.words) a.bits[P >> 5] = stg[(P >> 5) & 3];
+                if ((P & 31) && (P >> 5) < a.words) a.bits[P >> 5] = sh.carry;
                 const uint64_t gwe = (P >> 7) >> 3;
-                if (gwe < a.gap_words) a.gaps[gwe] = gst[0];
+                if (gwe < a.gap_words) a.gaps[gwe] = sh.gcarry[cons & 1];
                 if ((P + 31) / 32 != a.words || (P + 127) / 128 != a.segments) atomicOr(a.status, kDevSize);
             }
         }
+        if (warp == 0) {
+            cur = nxt;
+            agg_cur = agg_nxt;
+            if (cur < a.nst) claim_super_tile(a, lutl, lane, nxt, agg_nxt);
+            if (lane == 0) prod.run(a, ring, sh, cons, cur, nxt);
+        }
+    }
+
+    // every copy issued has been consumed, unless a wait gave up: never leave
+    // the CTA with a copy still in flight into its shared memory
+    if (tid == 0) {
+        const uint32_t first = prod.issued > (uint32_t)kRing ? prod.issued - kRing : 0u;
+        for (uint32_t i = first; i < prod.issued; ++i)
+            mbar_wait(&sh.mbar[i % kRing], (i / kRing) & 1, a.status, false);
     }
 }
 
