@@ -26,7 +26,10 @@ EXPORTS = [
     "hgap_encode_histogram", "hgap_encode_prepared",
     "hgap_decode_workspace_bytes", "hgap_decode", "hgap_workspace_status", "hgap_container_bytes",
     "hgap_container_write", "hgap_container_parse", "histgram", "hgap_ref_encode",
-    "hgap_ref_decoder_l1_l2", "hgap_decode_noalloc",
+    "hgap_ref_decoder_l1_l2", "hgap_decode_noalloc", "hgap_codebook_build_device",
+    "hgap_decode_table_build", "hgap_decode_table_build_device", "hgap_batch_compress_workspace_bytes",
+    "hgap_batch_decompress_workspace_bytes", "hgap_batch_bits_capacity", "hgap_batch_gaps_capacity",
+    "hgap_batch_compress", "hgap_batch_decompress", "hgap_batch_status",
 ]
 
 
@@ -51,6 +54,22 @@ class CCodebook(C.Structure):
 class Sizes(C.Structure):
     _fields_ = [("bits", C.c_uint64), ("words", C.c_uint64), ("segments", C.c_uint64),
                 ("gap_words", C.c_uint64)]
+
+
+class BatchEntry(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("bits", C.c_uint64), ("words", C.c_uint64),
+                ("segments", C.c_uint64), ("gap_words", C.c_uint64), ("bits_offset", C.c_uint64),
+                ("gaps_offset", C.c_uint64), ("symbol_count", C.c_uint32), ("status", C.c_uint32),
+                ("symbols", SymLen * 256)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("region_chunks", C.c_uint32), ("hist_ctas_per_sm", C.c_uint32),
+                ("enc_ctas_per_sm", C.c_uint32), ("dec_ctas_per_sm", C.c_uint32)]
+
+
+DEC_T1_ENTRIES = 2048
+DEC_T2_ENTRIES = 2560
 
 
 _lib = None
@@ -96,6 +115,26 @@ def lib() -> C.CDLL:
     L.hgap_ref_encode.argtypes = [vp, C.c_uint32, vp, C.c_uint32, C.c_uint32, C.POINTER(Codeword)]
     L.hgap_ref_decoder_l1_l2.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, vp, C.c_int, C.c_uint32,
                                          C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
+    u64p = C.POINTER(C.c_uint64)
+    L.hgap_codebook_build_device.argtypes = [C.c_uint32, vp, vp, vp, vp]
+    L.hgap_decode_table_build.argtypes = [C.POINTER(CCodebook), vp, vp]
+    L.hgap_decode_table_build_device.argtypes = [C.c_uint32, vp, vp, vp, vp]
+    L.hgap_batch_compress_workspace_bytes.argtypes = [C.c_uint32, u64p, C.POINTER(BatchConfig)]
+    L.hgap_batch_compress_workspace_bytes.restype = C.c_size_t
+    L.hgap_batch_decompress_workspace_bytes.argtypes = [C.c_uint32, u64p]
+    L.hgap_batch_decompress_workspace_bytes.restype = C.c_size_t
+    L.hgap_batch_bits_capacity.argtypes = [C.c_uint32, u64p]
+    L.hgap_batch_bits_capacity.restype = u64
+    L.hgap_batch_gaps_capacity.argtypes = [C.c_uint32, u64p]
+    L.hgap_batch_gaps_capacity.restype = u64
+    L.hgap_batch_compress.argtypes = [C.c_uint32, vp, vp, vp, vp, u64, vp, u64, vp, vp, C.c_size_t,
+                                      C.POINTER(BatchConfig), vp]
+    L.hgap_batch_decompress.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, C.c_size_t,
+                                        C.POINTER(BatchConfig), vp]
+    L.hgap_batch_status.argtypes = [vp, vp]
+    for name in ("hgap_codebook_build_device", "hgap_decode_table_build", "hgap_decode_table_build_device",
+                 "hgap_batch_compress", "hgap_batch_decompress", "hgap_batch_status"):
+        getattr(L, name).restype = C.c_int
     for name in ("hgap_histogram", "hgap_codebook_build", "hgap_codebook_from_symbols",
                  "hgap_encode", "hgap_encode_histogram", "hgap_encode_prepared", "hgap_decode", "hgap_workspace_status", "hgap_container_write",
                  "hgap_container_parse", "hgap_ref_encode", "hgap_ref_decoder_l1_l2",

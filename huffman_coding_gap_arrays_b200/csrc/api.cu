@@ -52,24 +52,28 @@ hgap_status encode_layout(const void* d_in, uint64_t n, void* d_workspace, size_
     const size_t need = hgap::kEncWsHeader + (size_t)nst * (sizeof(uint64_t) + 256 * sizeof(uint32_t));
     if (workspace_bytes < need) return HGAP_ERR_WORKSPACE;
     uint8_t* ws = static_cast<uint8_t*>(d_workspace);
-    a->in_aligned = reinterpret_cast<const uint8_t*>(addr - lo);
-    a->lo = lo;
-    a->hi = lo + n;
+    std::memset(a, 0, sizeof(*a));
+    std::memset(h, 0, sizeof(*h));
+    hgap::EncJob& J = a->single;
+    J.in_aligned = reinterpret_cast<const uint8_t*>(addr - lo);
+    J.lo = lo;
+    J.hi = lo + n;
+    J.item0 = 0;
+    J.nst = nst;
+    J.st_bytes = (uint32_t)st_bytes;
+    a->count = 1;
+    a->nitems = nst;
     a->status = reinterpret_cast<uint32_t*>(ws);
     a->counter = reinterpret_cast<uint32_t*>(ws) + 1;
     a->tag = reinterpret_cast<const uint64_t*>(ws + hgap::kEncWsTag);
     a->st_rec = reinterpret_cast<uint64_t*>(ws + hgap::kEncWsHeader);
     a->st_hist = reinterpret_cast<const uint32_t*>(a->st_rec + nst);
-    a->nst = nst;
-    a->st_bytes = (uint32_t)st_bytes;
-    h->in_aligned = a->in_aligned;
-    h->lo = lo;
-    h->hi = lo + n;
+    h->single = J;
+    h->count = 1;
+    h->nitems = nst;
     h->hist = reinterpret_cast<uint32_t*>(ws + hgap::kEncWsScratchHist);
     h->st_hist = const_cast<uint32_t*>(a->st_hist);
     h->tag = reinterpret_cast<uint64_t*>(ws + hgap::kEncWsTag);
-    h->nst = nst;
-    h->st_bytes = (uint32_t)st_bytes;
     return HGAP_OK;
 }
 
@@ -81,12 +85,13 @@ hgap_status encode_outputs(const hgap_codebook* cb, uint32_t* d_bits, uint64_t w
         const uint32_t l = cb->table[b].length;
         if (l > (uint32_t)hgap::kMaxLen || (l && (cb->table[b].code >> l) != 0)) return HGAP_ERR_CORRUPT;
     }
-    a->bits = d_bits;
-    a->words = words;
-    a->gaps = d_gaps;
-    a->segments = segments;
-    a->gap_words = (segments + 7) / 8;
-    a->bits_aligned16 = aligned(d_bits, 16) ? 1u : 0u;
+    hgap::EncJob& J = a->single;
+    J.bits = d_bits;
+    J.words = words;
+    J.gaps = d_gaps;
+    J.segments = segments;
+    J.gap_words = (segments + 7) / 8;
+    J.bits_aligned16 = aligned(d_bits, 16) ? 1u : 0u;
     return HGAP_OK;
 }
 
@@ -95,7 +100,7 @@ hgap_status encode_clear(const hgap::EncArgs& a, bool tag_too, cudaStream_t st) 
     uint8_t* ws = reinterpret_cast<uint8_t*>(a.status);
     if (cudaMemsetAsync(ws, 0, tag_too ? hgap::kEncWsHeader : hgap::kEncWsTag, st) != cudaSuccess)
         return HGAP_ERR_CUDA;
-    if (cudaMemsetAsync(a.st_rec, 0, sizeof(uint64_t) * a.nst, st) != cudaSuccess) return HGAP_ERR_CUDA;
+    if (cudaMemsetAsync(a.st_rec, 0, sizeof(uint64_t) * a.nitems, st) != cudaSuccess) return HGAP_ERR_CUDA;
     return HGAP_OK;
 }
 
@@ -115,7 +120,8 @@ hgap_status hgap_encode_histogram(const void* d_in, uint64_t n, uint32_t* d_hist
     h.hist = d_hist;
     s = encode_clear(a, true, st);
     if (s != HGAP_OK) return s;
-    return cuda_status(hgap::launch_hist_st(h, stream));
+    if (cudaMemsetAsync(d_hist, 0, 256 * sizeof(uint32_t), st) != cudaSuccess) return HGAP_ERR_CUDA;
+    return cuda_status(hgap::launch_hist_st(h, 0, stream));
 }
 
 hgap_status hgap_encode_prepared(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
@@ -133,7 +139,7 @@ hgap_status hgap_encode_prepared(const void* d_in, uint64_t n, const hgap_codebo
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     s = encode_clear(a, false, st);
     if (s != HGAP_OK) return s;
-    return cuda_status(hgap::launch_encode(a, t, stream));
+    return cuda_status(hgap::launch_encode(a, t, 0, stream));
 }
 
 hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
@@ -151,9 +157,10 @@ hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, u
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     s = encode_clear(a, true, st);
     if (s != HGAP_OK) return s;
-    int e = hgap::launch_hist_st(h, stream);  // per-super-tile histograms into the workspace
+    // per-region histograms into the workspace (the scratch histogram was cleared with the header)
+    int e = hgap::launch_hist_st(h, 0, stream);
     if (e != 0) return HGAP_ERR_CUDA;
-    return cuda_status(hgap::launch_encode(a, t, stream));
+    return cuda_status(hgap::launch_encode(a, t, 0, stream));
 }
 
 size_t hgap_decode_workspace_bytes(uint64_t segments) {
@@ -177,18 +184,23 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     s = hgap::make_dec_table(book, &t);
     if (s != HGAP_OK) return s;
     hgap::DecArgs a;
-    a.bits = d_bits;
-    a.words = words;
-    a.gaps = d_gaps;
-    a.segments = segments;
-    a.gap_words = (segments + 7) / 8;
+    std::memset(&a, 0, sizeof(a));
+    hgap::DecJob& J = a.single;
+    J.bits = d_bits;
+    J.words = words;
+    J.gaps = d_gaps;
+    J.segments = segments;
+    J.gap_words = (segments + 7) / 8;
     const uintptr_t addr = reinterpret_cast<uintptr_t>(d_out);
-    a.out_lo = addr & 15;
-    a.out_aligned = reinterpret_cast<uint8_t*>(addr - a.out_lo);
-    a.n = n;
-    a.ntiles = hgap::decode_tiles(segments);
-    if (a.ntiles >= 0xffffffffull) return HGAP_ERR_UNSUPPORTED;
-    const size_t need = kWsHeader + sizeof(uint64_t) * (size_t)a.ntiles;
+    J.out_lo = addr & 15;
+    J.out_aligned = reinterpret_cast<uint8_t*>(addr - J.out_lo);
+    J.n = n;
+    J.item0 = 0;
+    J.ntiles = hgap::decode_tiles(segments);
+    if (J.ntiles >= 0xffffffffull) return HGAP_ERR_UNSUPPORTED;
+    a.count = 1;
+    a.nitems = J.ntiles;
+    const size_t need = kWsHeader + sizeof(uint64_t) * (size_t)J.ntiles;
     if (workspace_bytes < need) return HGAP_ERR_WORKSPACE;
     uint8_t* ws = static_cast<uint8_t*>(d_workspace);
     a.status = reinterpret_cast<uint32_t*>(ws);
@@ -203,7 +215,7 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
         kraft += 1ull << (hgap::kMaxLen - book.symbols[i].length);
     }
     const bool complete = kraft == (1ull << hgap::kMaxLen);
-    return cuda_status(hgap::launch_decode(a, t, min_len, complete, stream));
+    return cuda_status(hgap::launch_decode(a, t, min_len, complete, 0, stream));
 }
 
 hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream) {

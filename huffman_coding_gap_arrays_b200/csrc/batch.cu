@@ -1,0 +1,615 @@
+// batch.cu -- the batched path (include/hgap.h, "batched path") and the
+// device-side codebook entry points.  No counterpart in the reference.
+//
+// Compress, all on the stream, nothing back to the host:
+//   1. benc_setup   one CTA: each buffer's alignment, region size and region
+//                   count; an exclusive scan numbers the regions globally;
+//   2. hist_st      per-region histograms and per-buffer histograms;
+//   3. book         one warp per buffer: length-limited canonical codebook,
+//                   encoder table, sizes (book.cuh);
+//   4. benc_place   one CTA: scans of the stream sizes place every bitstream
+//                   (16-byte aligned) and gap array in the two arenas;
+//   5. encode       the single-buffer encoder kernel over all regions, the
+//                   CTA reloading its code tables when the buffer changes.
+// Decompress:
+//   1. bdec_book    one warp per buffer: checks the book, builds its decoder
+//                   table, and puts the buffer in one of 8 classes (decoder
+//                   stage size by the shortest code x complete book or not);
+//   2. bdec_setup   one CTA: tiles per buffer, look-back record numbering,
+//                   and per class the numbering of the class's tiles;
+//   3. bdec_map     tile -> buffer map of each class;
+//   4. decode       one persistent launch per class (8), the single-buffer
+//                   decoder kernel over the class's tiles.
+// Every launch has a fixed grid and reads its work counts from device memory,
+// so the sequence can be captured once and replayed.
+#include <cuda_runtime.h>
+
+#include <cstring>
+
+#include "book.cuh"
+
+namespace hgap {
+namespace {
+
+constexpr int kBookWarps = 4;
+constexpr size_t kBookSmem = kBookWarps * sizeof(BookScratch);
+constexpr int kScanThreads = 1024;
+constexpr uint32_t kClasses = 8;
+constexpr uint32_t kNoClass = 0xffu;
+
+// ----------------------------------------------------------- block scans ---
+// Exclusive scan of one u64 per thread over a 1024-thread CTA; returns the
+// exclusive prefix and the block total.
+__device__ __forceinline__ uint64_t block_excl_scan_u64(uint64_t v, uint64_t* total, uint64_t* s_warp) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint64_t t = __shfl_up_sync(kFull, x, d);
+        if (lane >= (uint32_t)d) x += t;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint64_t w = s_warp[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint64_t t = __shfl_up_sync(kFull, w, d);
+            if (lane >= (uint32_t)d) w += t;
+        }
+        s_warp[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const uint64_t before = warp ? s_warp[warp - 1] : 0;
+    *total = s_warp[31];
+    __syncthreads();  // s_warp free for the next call
+    return before + x - v;
+}
+
+// --------------------------------------------------------------- compress ---
+
+__global__ void __launch_bounds__(kScanThreads) benc_setup_kernel(uint32_t count, const uint8_t* const* inputs,
+                                                                  const uint64_t* sizes,
+                                                                  const uint8_t* region_chunks,
+                                                                  uint32_t base_chunks, EncJob* jobs,
+                                                                  uint64_t* item0s, uint64_t* nitems,
+                                                                  uint64_t max_regions, uint32_t* status) {
+    __shared__ uint64_t s_warp[32];
+    uint64_t carry = 0;
+    for (uint32_t base = 0; base < count; base += kScanThreads) {
+        const uint32_t j = base + threadIdx.x;
+        uint64_t nst = 0, n = 0, lo = 0;
+        uint32_t st = 0;
+        const uint8_t* in = nullptr;
+        if (j < count) {
+            n = sizes[j];
+            in = inputs[j];
+            lo = reinterpret_cast<uintptr_t>(in) & 15;
+            uint32_t rc = region_chunks ? region_chunks[j] : base_chunks;
+            if (rc < base_chunks) rc = base_chunks;
+            if (rc > 32) rc = 32;
+            st = rc * (uint32_t)kEncChunkBytes;
+            nst = n ? (lo + n + st - 1) / st : 0;
+        }
+        uint64_t total = 0;
+        const uint64_t excl = block_excl_scan_u64(nst, &total, s_warp);
+        if (j < count) {
+            EncJob J;
+            memset(&J, 0, sizeof(J));
+            J.in_aligned = in - lo;
+            J.lo = lo;
+            J.hi = lo + n;
+            J.item0 = carry + excl;
+            J.nst = nst;
+            J.st_bytes = st;
+            jobs[j] = J;
+            item0s[j] = carry + excl;
+        }
+        carry += total;
+    }
+    if (threadIdx.x == 0) {
+        item0s[count] = carry;
+        // a workspace smaller than the query asked for: nothing is encoded
+        if (carry > max_regions) atomicOr(status, kDevSize);
+        *nitems = carry > max_regions ? 0 : carry;
+    }
+}
+
+// One warp per book: codebook from the buffer's histogram.  Optional outputs:
+// the public codebook, sizes, encoder table, batch entry.
+__global__ void __launch_bounds__(32 * kBookWarps) book_kernel(uint32_t count, const uint32_t* hists,
+                                                               hgap_codebook* books, hgap_sizes* sizes,
+                                                               EncTable* enc, hgap_batch_entry* entries,
+                                                               const uint64_t* in_sizes) {
+    extern __shared__ __align__(16) unsigned char book_smem[];
+    BookScratch& s = reinterpret_cast<BookScratch*>(book_smem)[threadIdx.x >> 5];
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t j = blockIdx.x * kBookWarps + (threadIdx.x >> 5); j < count; j += gridDim.x * kBookWarps) {
+        const uint32_t* h = hists + 256 * (uint64_t)j;
+        const uint32_t n = warp_code_lengths(h, s, lane);
+        warp_assign_codes(s, n, lane);
+        uint64_t part = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t b = lane + 32 * k;
+            part += (uint64_t)h[b] * s.blen[b];
+        }
+        const uint64_t bits = warp_sum_u64(part);
+        const uint64_t words = (bits + 31) / 32, segs = (bits + 127) / 128;
+        if (books) warp_write_book(s, n, books + j, lane);
+        if (enc) warp_write_enc_table(s, n, enc + j, lane);
+        if (sizes && lane == 0) {
+            sizes[j].bits = bits;
+            sizes[j].words = words;
+            sizes[j].segments = segs;
+            sizes[j].gap_words = (segs + 7) / 8;
+        }
+        if (entries) {
+            hgap_batch_entry& e = entries[j];
+            for (uint32_t c = lane; c < n; c += 32) {
+                e.symbols[c].symbol = s.sym[c];
+                e.symbols[c].length = s.clen[c];
+            }
+            if (lane == 0) {
+                e.n = in_sizes ? in_sizes[j] : 0;
+                e.bits = bits;
+                e.words = words;
+                e.segments = segs;
+                e.gap_words = (segs + 7) / 8;
+                e.symbol_count = n;
+                e.status = 0;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Places every stream in the arenas (bitstreams 16-byte aligned) and
+// completes the encoder jobs.
+__global__ void __launch_bounds__(kScanThreads) benc_place_kernel(uint32_t count, hgap_batch_entry* entries,
+                                                                  EncJob* jobs, uint32_t* bits,
+                                                                  uint64_t bits_cap, uint32_t* gaps,
+                                                                  uint64_t gaps_cap, uint32_t* status) {
+    __shared__ uint64_t s_warp[32];
+    uint64_t cb = 0, cg = 0;
+    for (uint32_t base = 0; base < count; base += kScanThreads) {
+        const uint32_t j = base + threadIdx.x;
+        uint64_t w = 0, g = 0;
+        if (j < count) {
+            w = (entries[j].words + 3) & ~3ull;
+            g = entries[j].gap_words;
+        }
+        uint64_t tb = 0, tg = 0;
+        const uint64_t ob = cb + block_excl_scan_u64(w, &tb, s_warp);
+        const uint64_t og = cg + block_excl_scan_u64(g, &tg, s_warp);
+        if (j < count) {
+            hgap_batch_entry& e = entries[j];
+            EncJob& J = jobs[j];
+            e.bits_offset = ob;
+            e.gaps_offset = og;
+            if (ob + e.words > bits_cap || og + e.gap_words > gaps_cap) {
+                e.status = HGAP_ERR_SIZE;  // the arena is too small: this stream is not written
+                atomicOr(status, kDevSize);
+                J.bits = bits;
+                J.words = 0;
+                J.gaps = gaps;
+                J.gap_words = 0;
+            } else {
+                J.bits = bits + ob;
+                J.words = e.words;
+                J.gaps = gaps + og;
+                J.gap_words = e.gap_words;
+            }
+            J.segments = e.segments;
+            J.bits_aligned16 = 1;
+        }
+        cb += tb;
+        cg += tg;
+    }
+}
+
+// ------------------------------------------------------------- decompress ---
+
+__device__ __forceinline__ uint32_t class_of(uint32_t min_len, bool complete) {
+    const uint32_t max_sym = (128 + min_len - 1) / min_len;
+    const uint32_t r = max_sym <= 32 ? 0 : max_sym <= 44 ? 1 : max_sym <= 64 ? 2 : 3;
+    return 2 * r + (complete ? 1 : 0);
+}
+
+__global__ void __launch_bounds__(32 * kBookWarps) bdec_book_kernel(uint32_t count,
+                                                                    const hgap_batch_entry* entries,
+                                                                    DecTable* tables, uint8_t* cls,
+                                                                    uint32_t* status) {
+    extern __shared__ __align__(16) unsigned char book_smem[];
+    BookScratch& s = reinterpret_cast<BookScratch*>(book_smem)[threadIdx.x >> 5];
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t j = blockIdx.x * kBookWarps + (threadIdx.x >> 5); j < count; j += gridDim.x * kBookWarps) {
+        const hgap_batch_entry& e = entries[j];
+        const uint32_t n = e.symbol_count;
+        uint32_t c = kNoClass;
+        bool bad = n > 256 || e.segments != (e.words + 3) / 4 || e.gap_words != (e.segments + 7) / 8 ||
+                   (e.n != 0) != (e.words != 0) || (e.n != 0 && n == 0);
+        if (!bad && n) {
+            const uint32_t kraft = warp_load_symbols(e.symbols, n, s, lane);
+            if (kraft == ~0u) {
+                bad = true;
+            } else if (!warp_dec_table(s, n, tables + j, lane)) {
+                bad = true;
+            } else {
+                c = class_of(s.clen[0], kraft == (1u << kMaxLen));
+            }
+        }
+        if (lane == 0) {
+            if (bad) {
+                atomicOr(status, kDevCorrupt);
+                c = kNoClass;
+            }
+            cls[j] = (uint8_t)c;
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count, const hgap_batch_entry* entries,
+                                                                  const uint8_t* cls, const uint32_t* bits,
+                                                                  const uint32_t* gaps, uint8_t* const* outputs,
+                                                                  DecJob* jobs, uint64_t* item0s,
+                                                                  uint64_t* class_nitems, uint64_t tiles_cap,
+                                                                  uint32_t* status) {
+    __shared__ uint64_t s_warp[32];
+    uint64_t carry = 0, ccarry[kClasses] = {};
+    for (uint32_t base = 0; base < count; base += kScanThreads) {
+        const uint32_t j = base + threadIdx.x;
+        uint64_t nt = 0;
+        uint32_t c = kNoClass;
+        if (j < count) {
+            c = cls[j];
+            if (c != kNoClass) nt = (entries[j].segments + 511) / 512;
+        }
+        uint64_t total = 0;
+        const uint64_t rec0 = carry + block_excl_scan_u64(nt, &total, s_warp);
+        carry += total;
+        for (uint32_t k = 0; k < kClasses; ++k) {
+            uint64_t tk = 0;
+            const uint64_t i0 = ccarry[k] + block_excl_scan_u64(c == k ? nt : 0, &tk, s_warp);
+            if (j < count) item0s[(uint64_t)k * (count + 1) + j] = i0;
+            ccarry[k] += tk;
+        }
+        if (j < count) {
+            const hgap_batch_entry& e = entries[j];
+            DecJob J;
+            memset(&J, 0, sizeof(J));
+            J.bits = bits + e.bits_offset;
+            J.words = e.words;
+            J.gaps = gaps + e.gaps_offset;
+            J.gap_words = e.gap_words;
+            J.segments = e.segments;
+            uint8_t* out = outputs[j];
+            J.out_lo = reinterpret_cast<uintptr_t>(out) & 15;
+            J.out_aligned = out - J.out_lo;
+            J.n = e.n;
+            J.item0 = rec0;
+            J.ntiles = nt;
+            jobs[j] = J;
+        }
+    }
+    // a workspace smaller than the query asked for: nothing is decoded
+    const bool fits = carry <= tiles_cap;
+    if (threadIdx.x == 0 && !fits) atomicOr(status, kDevSize);
+    if (threadIdx.x < kClasses) {
+        item0s[(uint64_t)threadIdx.x * (count + 1) + count] = ccarry[threadIdx.x];
+        class_nitems[threadIdx.x] = fits ? ccarry[threadIdx.x] : 0;
+    }
+}
+
+// tile -> job map of each class: job_of[k * cap + item] = job
+__global__ void bdec_map_kernel(uint32_t count, const DecJob* jobs, const uint8_t* cls, const uint64_t* item0s,
+                                uint32_t* job_of, uint64_t cap) {
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); j < count;
+         j += gridDim.x * (blockDim.x >> 5)) {
+        const uint32_t c = cls[j];
+        if (c == kNoClass) continue;
+        const uint64_t i0 = item0s[(uint64_t)c * (count + 1) + j];
+        const uint64_t nt = jobs[j].ntiles;
+        for (uint64_t t = lane; t < nt; t += 32)
+            if (i0 + t < cap) job_of[(uint64_t)c * cap + i0 + t] = j;
+    }
+}
+
+// One warp per book: the decoder table of a public codebook.
+__global__ void __launch_bounds__(32 * kBookWarps) dec_table_kernel(uint32_t count, const hgap_codebook* books,
+                                                                    uint16_t* tables, uint32_t* status) {
+    extern __shared__ __align__(16) unsigned char book_smem[];
+    BookScratch& s = reinterpret_cast<BookScratch*>(book_smem)[threadIdx.x >> 5];
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t j = blockIdx.x * kBookWarps + (threadIdx.x >> 5); j < count; j += gridDim.x * kBookWarps) {
+        const uint32_t n = books[j].symbol_count;
+        DecTable* t = reinterpret_cast<DecTable*>(tables + (uint64_t)j * (HGAP_DEC_T1_ENTRIES + HGAP_DEC_T2_ENTRIES));
+        bool ok = n >= 1 && n <= 256;
+        if (ok) {
+            const uint32_t kraft = warp_load_symbols(books[j].symbols, n, s, lane);
+            ok = kraft != ~0u && warp_dec_table(s, n, t, lane);
+        }
+        if (!ok && lane == 0 && status) atomicOr(status + j, 1u);
+        __syncwarp();
+    }
+}
+
+// --------------------------------------------------------- host helpers ---
+
+int sm_count() {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    return sms;
+}
+
+template <class K>
+cudaError_t set_book_smem(K kern) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBookSmem);
+}
+
+unsigned book_grid(uint32_t count) {
+    const uint64_t want = (count + kBookWarps - 1) / kBookWarps;
+    const uint64_t cap = (uint64_t)sm_count() * 8;
+    return (unsigned)(want < cap ? (want ? want : 1) : cap);
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+uint32_t base_chunks(const hgap_batch_config* cfg) {
+    uint32_t rc = cfg && cfg->region_chunks ? cfg->region_chunks : 8;
+    return rc > 32 ? 32 : rc;
+}
+
+// Compress workspace: [header 1024: status @0, counter @4, nitems @64]
+// [jobs] [item0s] [tables] [hists] then the per-region arrays [st_rec | st_hist]
+// for as many regions as the rest of the workspace holds.
+constexpr size_t kEncPerRegion = 8 + 1024;
+
+struct EncLayout {
+    size_t jobs, item0s, tables, hists, st_rec, st_hist, fixed;
+    uint64_t max_regions;
+};
+
+EncLayout enc_layout(uint32_t count, size_t workspace_bytes) {
+    EncLayout L;
+    size_t off = 1024;
+    L.jobs = off;
+    off = align256(off + sizeof(EncJob) * (size_t)count);
+    L.item0s = off;
+    off = align256(off + 8 * ((size_t)count + 1));
+    L.tables = off;
+    off = align256(off + sizeof(EncTable) * (size_t)count);
+    L.hists = off;
+    off = align256(off + 1024 * (size_t)count);
+    L.fixed = off;
+    L.max_regions = workspace_bytes > off + 256 ? (workspace_bytes - off - 256) / kEncPerRegion : 0;
+    L.st_rec = off;
+    L.st_hist = align256(off + 8 * (size_t)L.max_regions);
+    return L;
+}
+
+uint64_t worst_regions(uint32_t count, const uint64_t* sizes, const hgap_batch_config* cfg) {
+    const uint64_t st = (uint64_t)base_chunks(cfg) * kEncChunkBytes;
+    uint64_t r = 0;
+    for (uint32_t j = 0; j < count; ++j) r += sizes[j] ? (sizes[j] + 15 + st - 1) / st : 0;
+    return r;
+}
+
+// Decompress workspace: [header 1024: status @0, counters[8] @64, class nitems[8] @128]
+// [jobs] [tables] [classes] [item0s 8 x (count+1)] then the per-tile arrays
+// [records | job_of 8 x cap] for as many tiles as the rest holds.
+constexpr size_t kDecPerTile = 8 + 4 * kClasses;
+
+struct DecLayout {
+    size_t jobs, tables, cls, item0s, records, job_of, fixed;
+    uint64_t tiles_cap;
+};
+
+DecLayout dec_layout(uint32_t count, size_t workspace_bytes) {
+    DecLayout L;
+    size_t off = 1024;
+    L.jobs = off;
+    off = align256(off + sizeof(DecJob) * (size_t)count);
+    L.tables = off;
+    off = align256(off + sizeof(DecTable) * (size_t)count);
+    L.cls = off;
+    off = align256(off + (size_t)count);
+    L.item0s = off;
+    off = align256(off + 8 * (size_t)kClasses * ((size_t)count + 1));
+    L.fixed = off;
+    L.tiles_cap = workspace_bytes > off + 256 ? (workspace_bytes - off - 256) / kDecPerTile : 0;
+    L.records = off;
+    L.job_of = align256(off + 8 * (size_t)L.tiles_cap);
+    return L;
+}
+
+uint64_t worst_tiles(uint32_t count, const uint64_t* sizes) {
+    uint64_t cap = 0;  // a stream has at most ceil(n / 8) segments (16-bit codes): ceil(n / 4096) tiles
+    for (uint32_t j = 0; j < count; ++j) cap += (sizes[j] + 4095) / 4096;
+    return cap;
+}
+
+inline hgap_status cuda_status(int e) { return e == 0 ? HGAP_OK : HGAP_ERR_CUDA; }
+
+}  // namespace
+}  // namespace hgap
+
+using namespace hgap;
+
+extern "C" {
+
+hgap_status hgap_codebook_build_device(uint32_t count, const uint32_t* d_hists, hgap_codebook* d_books,
+                                       hgap_sizes* d_sizes, hgap_stream_t stream) {
+    if (count == 0) return HGAP_OK;
+    if (!d_hists || !d_books) return HGAP_ERR_INVALID_ARG;
+    if (set_book_smem(book_kernel) != cudaSuccess) return HGAP_ERR_CUDA;
+    book_kernel<<<book_grid(count), 32 * kBookWarps, kBookSmem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        count, d_hists, d_books, d_sizes, nullptr, nullptr, nullptr);
+    return cuda_status(cudaGetLastError());
+}
+
+hgap_status hgap_decode_table_build_device(uint32_t count, const hgap_codebook* d_books, uint16_t* d_tables,
+                                           uint32_t* d_status, hgap_stream_t stream) {
+    if (count == 0) return HGAP_OK;
+    if (!d_books || !d_tables) return HGAP_ERR_INVALID_ARG;
+    if (set_book_smem(dec_table_kernel) != cudaSuccess) return HGAP_ERR_CUDA;
+    dec_table_kernel<<<book_grid(count), 32 * kBookWarps, kBookSmem, reinterpret_cast<cudaStream_t>(stream)>>>(
+        count, d_books, d_tables, d_status);
+    return cuda_status(cudaGetLastError());
+}
+
+size_t hgap_batch_compress_workspace_bytes(uint32_t count, const uint64_t* sizes, const hgap_batch_config* cfg) {
+    if (count && !sizes) return 0;
+    const EncLayout L = enc_layout(count, 0);
+    return L.fixed + 256 + kEncPerRegion * (size_t)worst_regions(count, sizes, cfg) + 256;
+}
+
+size_t hgap_batch_decompress_workspace_bytes(uint32_t count, const uint64_t* sizes) {
+    if (count && !sizes) return 0;
+    const DecLayout L = dec_layout(count, 0);
+    return L.fixed + 256 + kDecPerTile * (size_t)worst_tiles(count, sizes) + 256;
+}
+
+uint64_t hgap_batch_bits_capacity(uint32_t count, const uint64_t* sizes) {
+    uint64_t w = 0;  // at most 16 bits per byte, each stream rounded up to 4 words
+    for (uint32_t j = 0; j < count; ++j) w += ((sizes[j] * 16 + 31) / 32 + 3) & ~3ull;
+    return w;
+}
+
+uint64_t hgap_batch_gaps_capacity(uint32_t count, const uint64_t* sizes) {
+    uint64_t g = 0;
+    for (uint32_t j = 0; j < count; ++j) g += ((sizes[j] * 16 + 127) / 128 + 7) / 8;
+    return g;
+}
+
+hgap_status hgap_batch_compress(uint32_t count, const uint8_t* const* d_inputs, const uint64_t* d_sizes,
+                                const uint8_t* d_region_chunks, uint32_t* d_bits, uint64_t bits_capacity,
+                                uint32_t* d_gaps, uint64_t gaps_capacity, hgap_batch_entry* d_entries,
+                                void* d_workspace, size_t workspace_bytes, const hgap_batch_config* cfg,
+                                hgap_stream_t stream) {
+    if (count == 0) return HGAP_OK;
+    if (!d_inputs || !d_sizes || !d_bits || !d_gaps || !d_entries || !d_workspace) return HGAP_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(d_workspace) & 255) || (reinterpret_cast<uintptr_t>(d_bits) & 15) ||
+        (reinterpret_cast<uintptr_t>(d_gaps) & 3))
+        return HGAP_ERR_INVALID_ARG;
+    const hgap_batch_config dflt = {0, 0, 0, 0};
+    if (!cfg) cfg = &dflt;
+    const EncLayout L = enc_layout(count, workspace_bytes);
+    if (L.max_regions == 0) return HGAP_ERR_WORKSPACE;
+    uint8_t* ws = static_cast<uint8_t*>(d_workspace);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t* status = reinterpret_cast<uint32_t*>(ws);
+    uint64_t* nitems = reinterpret_cast<uint64_t*>(ws + 64);
+    EncJob* jobs = reinterpret_cast<EncJob*>(ws + L.jobs);
+    uint64_t* item0s = reinterpret_cast<uint64_t*>(ws + L.item0s);
+    EncTable* tables = reinterpret_cast<EncTable*>(ws + L.tables);
+    uint32_t* hists = reinterpret_cast<uint32_t*>(ws + L.hists);
+    uint64_t* st_rec = reinterpret_cast<uint64_t*>(ws + L.st_rec);
+    uint32_t* st_hist = reinterpret_cast<uint32_t*>(ws + L.st_hist);
+
+    if (cudaMemsetAsync(ws, 0, 1024, st) != cudaSuccess) return HGAP_ERR_CUDA;
+    if (cudaMemsetAsync(hists, 0, 1024 * (size_t)count, st) != cudaSuccess) return HGAP_ERR_CUDA;
+    benc_setup_kernel<<<1, kScanThreads, 0, st>>>(count, d_inputs, d_sizes, d_region_chunks, base_chunks(cfg), jobs,
+                                                  item0s, nitems, L.max_regions, status);
+    if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
+    if (cudaMemsetAsync(st_rec, 0, 8 * (size_t)L.max_regions, st) != cudaSuccess) return HGAP_ERR_CUDA;
+
+    HistStArgs h;
+    std::memset(&h, 0, sizeof(h));
+    h.jobs = jobs;
+    h.item0s = item0s;
+    h.count = count;
+    h.nitems_dev = nitems;
+    h.hist = hists;
+    h.st_hist = st_hist;
+    if (launch_hist_st(h, (int)cfg->hist_ctas_per_sm, stream) != 0) return HGAP_ERR_CUDA;
+
+    if (set_book_smem(book_kernel) != cudaSuccess) return HGAP_ERR_CUDA;
+    book_kernel<<<book_grid(count), 32 * kBookWarps, kBookSmem, st>>>(count, hists, nullptr, nullptr, tables,
+                                                                      d_entries, d_sizes);
+    if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
+    benc_place_kernel<<<1, kScanThreads, 0, st>>>(count, d_entries, jobs, d_bits, bits_capacity, d_gaps,
+                                                  gaps_capacity, status);
+    if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
+
+    EncArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.jobs = jobs;
+    a.item0s = item0s;
+    a.tables = tables;
+    a.count = count;
+    a.nitems_dev = nitems;
+    a.st_rec = st_rec;
+    a.st_hist = st_hist;
+    a.counter = status + 1;
+    a.status = status;
+    EncTable unused;
+    std::memset(&unused, 0, sizeof(unused));
+    return cuda_status(launch_encode(a, unused, (int)cfg->enc_ctas_per_sm, stream));
+}
+
+hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entries, const uint32_t* d_bits,
+                                  const uint32_t* d_gaps, uint8_t* const* d_outputs, void* d_workspace,
+                                  size_t workspace_bytes, const hgap_batch_config* cfg, hgap_stream_t stream) {
+    if (count == 0) return HGAP_OK;
+    if (!d_entries || !d_bits || !d_gaps || !d_outputs || !d_workspace) return HGAP_ERR_INVALID_ARG;
+    if (reinterpret_cast<uintptr_t>(d_workspace) & 255) return HGAP_ERR_INVALID_ARG;
+    const hgap_batch_config dflt = {0, 0, 0, 0};
+    if (!cfg) cfg = &dflt;
+    const DecLayout L = dec_layout(count, workspace_bytes);
+    if (L.tiles_cap == 0) return HGAP_ERR_WORKSPACE;
+    uint8_t* ws = static_cast<uint8_t*>(d_workspace);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t* status = reinterpret_cast<uint32_t*>(ws);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(ws + 64);
+    uint64_t* class_nitems = reinterpret_cast<uint64_t*>(ws + 128);
+    DecJob* jobs = reinterpret_cast<DecJob*>(ws + L.jobs);
+    DecTable* tables = reinterpret_cast<DecTable*>(ws + L.tables);
+    uint8_t* cls = ws + L.cls;
+    uint64_t* item0s = reinterpret_cast<uint64_t*>(ws + L.item0s);
+    uint64_t* records = reinterpret_cast<uint64_t*>(ws + L.records);
+    uint32_t* job_of = reinterpret_cast<uint32_t*>(ws + L.job_of);
+
+    if (cudaMemsetAsync(ws, 0, 1024, st) != cudaSuccess) return HGAP_ERR_CUDA;
+    if (set_book_smem(bdec_book_kernel) != cudaSuccess) return HGAP_ERR_CUDA;
+    bdec_book_kernel<<<book_grid(count), 32 * kBookWarps, kBookSmem, st>>>(count, d_entries, tables, cls, status);
+    if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
+    bdec_setup_kernel<<<1, kScanThreads, 0, st>>>(count, d_entries, cls, d_bits, d_gaps, d_outputs, jobs, item0s,
+                                                  class_nitems, L.tiles_cap, status);
+    if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
+    bdec_map_kernel<<<book_grid(count), 32 * kBookWarps, 0, st>>>(count, jobs, cls, item0s, job_of, L.tiles_cap);
+    if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
+    if (cudaMemsetAsync(records, 0, 8 * (size_t)L.tiles_cap, st) != cudaSuccess) return HGAP_ERR_CUDA;
+
+    DecTable unused;
+    std::memset(&unused, 0, sizeof(unused));
+    static const uint32_t kMinLen[4] = {4, 3, 2, 1};  // a representative shortest code per stage size
+    for (uint32_t c = 0; c < kClasses; ++c) {
+        DecArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.jobs = jobs;
+        a.job_of = job_of + (uint64_t)c * L.tiles_cap;
+        a.item0s = item0s + (uint64_t)c * (count + 1);
+        a.tables = tables;
+        a.count = count;
+        a.nitems_dev = class_nitems + c;
+        a.lookback = records;
+        a.counter = counters + c;
+        a.status = status;
+        if (launch_decode(a, unused, kMinLen[c / 2], (c & 1) != 0, (int)cfg->dec_ctas_per_sm, stream) != 0)
+            return HGAP_ERR_CUDA;
+    }
+    return HGAP_OK;
+}
+
+hgap_status hgap_batch_status(const void* d_workspace, hgap_stream_t stream) {
+    return hgap_workspace_status(d_workspace, stream);
+}
+
+}  // extern "C"

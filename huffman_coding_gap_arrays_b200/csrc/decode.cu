@@ -73,11 +73,20 @@ __device__ __forceinline__ uint32_t lookup(const uint32_t* sw, const uint32_t* t
     return e;
 }
 
+// A claimed tile and its job, in shared memory.
+struct DecSlot {
+    DecJob job;
+    uint64_t item;    // tile id in the launch's numbering (>= nitems: none)
+    uint64_t local;   // tile index within its job
+    uint32_t job_id;
+    uint32_t pad;
+};
+
 // COMPLETE: the book's Kraft sum is 1 (every package-merge book with two or
 // more symbols), so no table entry is invalid and the decode loop skips that test.
 template <int R, bool COMPLETE>
 __global__ void __launch_bounds__(kDecThreads, 3)
-    decode_kernel(const DecArgs a, const __grid_constant__ DecTable tab) {
+    decode_kernel(const __grid_constant__ DecArgs a, const __grid_constant__ DecTable tab) {
     using C = DecCfg<R>;
     extern __shared__ __align__(16) uint32_t smem[];
     uint32_t* t1 = smem;
@@ -87,28 +96,44 @@ __global__ void __launch_bounds__(kDecThreads, 3)
     uint8_t* stage = reinterpret_cast<uint8_t*>(sg + C::kGapStage);
     uint8_t* compact = stage + C::kStageBytes;
     __shared__ uint32_t warp_tot[C::kWarps];
-    __shared__ uint64_t s_tile[2];
+    __shared__ DecSlot slot[3];  // ring: the tile being decoded, the next one, the previous one
     __shared__ uint64_t s_O;
+    __shared__ uint64_t s_nitems;
+    __shared__ uint32_t s_lut_job;
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < C::kT1; i += kDecThreads) t1[i] = widen_entry(tab.t1[i]);
-    for (int i = tid; i < C::kT2; i += kDecThreads) t2[i] = tab.t2[i];
-    const uint64_t stream_bits = a.words * 32;
+    auto load_tables = [&](const DecTable& t) {
+        for (int i = tid; i < C::kT1; i += kDecThreads) t1[i] = widen_entry(t.t1[i]);
+        for (int i = tid; i < C::kT2; i += kDecThreads) t2[i] = t.t2[i];
+    };
+    // thread 0: the tile `item` and its job into slot s
+    auto fill_slot = [&](int s, uint64_t item) {
+        DecSlot& d = slot[s];
+        d.item = item;
+        if (item < s_nitems) {
+            const uint32_t j = a.jobs ? a.job_of[item] : 0u;
+            d.job = a.jobs ? a.jobs[j] : a.single;
+            d.local = a.jobs ? item - a.item0s[j] : item;
+            d.job_id = j;
+        }
+    };
 
     // Loads of one tile's bitstream words and gap words into registers
     // (issued a tile ahead) and their store into shared memory.
-#define HGAP_PREFETCH(T)                                                                      \
+#define HGAP_PREFETCH(S)                                                                      \
     do {                                                                                      \
-        const uint64_t ps0 = (T) * kDecSegs;                                                  \
+        const DecSlot& ps = slot[S];                                                          \
+        const bool ok = ps.item < s_nitems;                                                   \
+        const uint64_t ps0 = ps.local * kDecSegs;                                             \
         _Pragma("unroll") for (int j = 0; j < C::kWordsPer; ++j) {                            \
             const uint32_t i = tid + j * kDecThreads;                                         \
             const uint64_t w = 4 * ps0 + i;                                                   \
-            pre[j] = ((T) < a.ntiles && i < (uint32_t)C::kWords && w < a.words)               \
-                         ? ld_stream_u32(a.bits + w) : 0u;                                    \
+            pre[j] = (ok && i < (uint32_t)C::kWords && w < ps.job.words)                      \
+                         ? ld_stream_u32(ps.job.bits + w) : 0u;                               \
         }                                                                                     \
         const int64_t g = (int64_t)(ps0 / 8) - 1 + (int64_t)tid;                              \
-        pre_gap = ((T) < a.ntiles && tid < (uint32_t)C::kGapStage && g >= 0 &&                \
-                   (uint64_t)g < a.gap_words) ? __ldg(a.gaps + g) : 0u;                       \
+        pre_gap = (ok && tid < (uint32_t)C::kGapStage && g >= 0 &&                            \
+                   (uint64_t)g < ps.job.gap_words) ? __ldg(ps.job.gaps + g) : 0u;             \
     } while (0)
 #define HGAP_COMMIT()                                                                         \
     do {                                                                                      \
@@ -119,23 +144,35 @@ __global__ void __launch_bounds__(kDecThreads, 3)
         if (tid < (uint32_t)C::kGapStage) sg[tid] = pre_gap;                                  \
     } while (0)
 
+    if (!a.jobs) load_tables(tab);
+    if (tid == 0) {
+        s_nitems = a.nitems_dev ? *a.nitems_dev : a.nitems;
+        fill_slot(0, atomicAdd(a.counter, 1u));
+        s_lut_job = a.jobs ? ~0u : 0u;
+    }
+    __syncthreads();
+    if (a.jobs && slot[0].item < s_nitems) load_tables(a.tables[slot[0].job_id]);
     uint32_t pre[C::kWordsPer];
     uint32_t pre_gap = 0;
-    if (tid == 0) s_tile[0] = atomicAdd(a.counter, 1u);
-    __syncthreads();
-    uint64_t tile = s_tile[0];
-    HGAP_PREFETCH(tile);
+    HGAP_PREFETCH(0);
     HGAP_COMMIT();
-    uint32_t parity = 0;
-    // The tile decoded one iteration earlier: its symbols wait in `compact`
-    // (at tile-local offsets) until its output offset is resolved.
-    uint64_t prev = ~0ull;
+    int ti = 0;        // slot of the tile decoded in this iteration
+    int prev_s = -1;   // slot of the tile decoded one iteration earlier: its symbols wait in
+                       // `compact` (at tile-local offsets) until its output offset is resolved
     uint32_t prev_ct = 0;
 
-    while (tile < a.ntiles || prev != ~0ull) {
-        __syncthreads();  // (1) words of `tile` staged; `compact` holds `prev`
-        const bool have = tile < a.ntiles;
-        const uint64_t s0 = tile * kDecSegs;
+    for (;;) {
+        __syncthreads();  // (1) words of the tile staged, its tables loaded; `compact` holds prev
+        const DecSlot& T = slot[ti];
+        const bool have = T.item < s_nitems;
+        if (!have && prev_s < 0) break;
+        if (tid == 0 && have) s_lut_job = T.job_id;
+        const int ns = ti == 2 ? 0 : ti + 1;  // slot of the next tile
+        uint32_t claim = 0;
+        if (tid == 0 && have) claim = atomicAdd(a.counter, 1u);  // its latency hides behind the decode
+        const uint64_t s0 = T.local * kDecSegs;  // first segment of the tile within its job
+        const uint64_t segments = T.job.segments;
+        const uint64_t stream_bits = T.job.words * 32;
         auto gap_of = [&](uint64_t k) -> uint32_t {  // k in [s0 - 1, s0 + 512)
             const uint32_t j = (uint32_t)((k >> 3) - (s0 >> 3) + 1);
             return (sg[j] >> (4 * (uint32_t)(k & 7))) & 0xfu;
@@ -149,8 +186,8 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                 const uint32_t col = tid + k * kDecThreads;
                 const uint64_t s = s0 + col;
                 uint32_t cnt = 0;
-                if (s < a.segments) {
-                    const bool last = s + 1 == a.segments;
+                if (s < segments) {
+                    const bool last = s + 1 == segments;
                     uint32_t pos = 128 * col + (s ? gap_of(s - 1) : 0u);
                     uint32_t end = 128 * col + 128;
                     if (last && stream_bits - 128 * s0 < end) end = (uint32_t)(stream_bits - 128 * s0);
@@ -180,9 +217,13 @@ __global__ void __launch_bounds__(kDecThreads, 3)
         const uint32_t i0 = warp_incl_scan(n[0], lane);
         const uint32_t i1 = warp_incl_scan(n[1], lane);
         if (lane == 31) warp_tot[warp] = i0 | (i1 << 16);  // a warp's 32 segments: < 2^13 symbols
-        if (tid == 0 && have) s_tile[parity ^ 1] = atomicAdd(a.counter, 1u);
-        __syncthreads();  // (2) decode done; next tile id known
-        const uint64_t next = have ? s_tile[parity ^ 1] : ~0ull;
+        if (tid == 0) {
+            if (have) fill_slot(ns, claim);
+            else slot[ns].item = ~0ull;
+        }
+        __syncthreads();  // (2) decode done; next tile known
+        const DecSlot& N = slot[ns];
+        const bool have_next = N.item < s_nitems;
         uint32_t wt = lane < (uint32_t)C::kWarps ? warp_tot[lane] : 0u;
         uint32_t w0 = warp_incl_scan(wt & 0xffffu, lane), w1 = warp_incl_scan(wt >> 16, lane);
         const uint32_t total0 = __shfl_sync(kFull, w0, C::kWarps - 1);
@@ -191,23 +232,28 @@ __global__ void __launch_bounds__(kDecThreads, 3)
         const uint32_t before1 = warp ? __shfl_sync(kFull, w1, warp - 1) : 0u;
         const uint32_t Ct = total0 + total1;
         const uint32_t excl[2] = {before0 + i0 - n[0], total0 + before1 + i1 - n[1]};
-        if (tid == 0 && have) lookback_publish(a.lookback, tile, Ct);
-        if (next < a.ntiles) HGAP_PREFETCH(next);  // in flight while `prev` is resolved and written
-        if (prev != ~0ull && warp == 0) {
-            const uint64_t O = lookback_resolve<kDecLookK>(a.lookback, prev, prev_ct, a.status, lane);
+        if (tid == 0 && have) lookback_publish(a.lookback, T.job.item0 + T.local, Ct, T.local == 0);
+        if (have_next) HGAP_PREFETCH(ns);  // in flight while prev is resolved and written
+        if (prev_s >= 0 && warp == 0) {
+            const DecSlot& Pv = slot[prev_s];
+            const uint64_t O =
+                lookback_resolve<kDecLookK>(a.lookback, Pv.job.item0 + Pv.local, prev_ct, Pv.local == 0, a.status, lane);
             if (lane == 0) s_O = O;
         }
         __syncthreads();  // (3) prev's output offset known
 
-        // ---- 3. write out `prev`: 16-byte output chunk q takes compact bytes
+        // ---- 3. write out prev: 16-byte output chunk q takes compact bytes
         //         [16q - vstart, 16q - vstart + 16), i.e. parts of two aligned groups
-        if (prev != ~0ull) {
+        if (prev_s >= 0) {
+            const DecSlot& Pv = slot[prev_s];
             const uint64_t O = s_O;
             const uint32_t Cp = prev_ct;
-            if (tid == 0 && prev + 1 == a.ntiles && O + Cp < a.n) atomicOr(a.status, kDevSize);
-            if (O < a.n) {
-                const uint64_t vstart = a.out_lo + O;
-                const uint64_t vend = a.out_lo + (O + Cp < a.n ? O + Cp : a.n);
+            const uint64_t nout = Pv.job.n;
+            uint8_t* const out_al = Pv.job.out_aligned;
+            if (tid == 0 && Pv.local + 1 == Pv.job.ntiles && O + Cp < nout) atomicOr(a.status, kDevSize);
+            if (O < nout) {
+                const uint64_t vstart = Pv.job.out_lo + O;
+                const uint64_t vend = Pv.job.out_lo + (O + Cp < nout ? O + Cp : nout);
                 const uint32_t base = (uint32_t)(vstart & 15);  // compact byte 0 sits at chunk offset base
                 const uint64_t q0 = vstart >> 4, q1 = (vend + 15) >> 4;
                 const uint32_t nq = (uint32_t)(q1 - q0);
@@ -236,12 +282,12 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                     }
                     const uint64_t c0 = (q0 + lq) << 4;
                     if (c0 >= vstart && c0 + 16 <= vend) {
-                        *reinterpret_cast<uint4*>(a.out_aligned + c0) = make_uint4(o[0], o[1], o[2], o[3]);
+                        *reinterpret_cast<uint4*>(out_al + c0) = make_uint4(o[0], o[1], o[2], o[3]);
                     } else {
 #pragma unroll
                         for (uint32_t b = 0; b < 16; ++b) {
                             const uint64_t vb = c0 + b;
-                            if (vb >= vstart && vb < vend) a.out_aligned[vb] = (uint8_t)(o[b >> 2] >> (8 * (b & 3)));
+                            if (vb >= vstart && vb < vend) out_al[vb] = (uint8_t)(o[b >> 2] >> (8 * (b & 3)));
                         }
                     }
                 }
@@ -258,11 +304,13 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                 for (uint32_t j = 0; j < n[k]; ++j) dst[j] = src[j * C::kPitch];
             }
         }
-        if (next < a.ntiles) HGAP_COMMIT();  // sw/sg are no longer read for this tile
-        prev = have ? tile : ~0ull;
+        if (have_next) {  // sw/sg and the tables are no longer read for this tile
+            if (a.jobs && N.job_id != s_lut_job) load_tables(a.tables[N.job_id]);
+            HGAP_COMMIT();
+        }
+        prev_s = have ? ti : -1;
         prev_ct = Ct;
-        tile = have ? next : ~0ull;
-        parity ^= 1;
+        ti = ns;
     }
 #undef HGAP_PREFETCH
 #undef HGAP_COMMIT
@@ -271,7 +319,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
 uint64_t decode_tiles(uint64_t segments) { return (segments + kDecSegs - 1) / kDecSegs; }
 
 template <int R, bool COMPLETE>
-static int launch_decode_r(const DecArgs& a, const DecTable& t, cudaStream_t st) {
+static int launch_decode_r(const DecArgs& a, const DecTable& t, int ctas_per_sm, cudaStream_t st) {
     using C = DecCfg<R>;
     auto kern = decode_kernel<R, COMPLETE>;
     static int sms = 0, per_sm = 0;
@@ -284,26 +332,29 @@ static int launch_decode_r(const DecArgs& a, const DecTable& t, cudaStream_t st)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kDecThreads, C::kSmem);
         if (per_sm < 1) per_sm = 1;
     }
-    const uint64_t cap = (uint64_t)sms * per_sm;
-    const unsigned grid = (unsigned)(a.ntiles < cap ? a.ntiles : cap);
+    const int k = (ctas_per_sm > 0 && ctas_per_sm < per_sm) ? ctas_per_sm : per_sm;
+    const uint64_t cap = (uint64_t)sms * k;
+    const unsigned grid = (unsigned)(a.nitems_dev ? cap : (a.nitems < cap ? (a.nitems ? a.nitems : 1) : cap));
     kern<<<grid, kDecThreads, C::kSmem, st>>>(a, t);
     return cudaGetLastError();
 }
 
 template <bool COMPLETE>
-static int launch_decode_c(const DecArgs& a, const DecTable& t, uint32_t max_sym, cudaStream_t st) {
-    if (max_sym <= 32) return launch_decode_r<8, COMPLETE>(a, t, st);
-    if (max_sym <= 44) return launch_decode_r<11, COMPLETE>(a, t, st);
-    if (max_sym <= 64) return launch_decode_r<16, COMPLETE>(a, t, st);
-    return launch_decode_r<32, COMPLETE>(a, t, st);
+static int launch_decode_c(const DecArgs& a, const DecTable& t, uint32_t max_sym, int k, cudaStream_t st) {
+    if (max_sym <= 32) return launch_decode_r<8, COMPLETE>(a, t, k, st);
+    if (max_sym <= 44) return launch_decode_r<11, COMPLETE>(a, t, k, st);
+    if (max_sym <= 64) return launch_decode_r<16, COMPLETE>(a, t, k, st);
+    return launch_decode_r<32, COMPLETE>(a, t, k, st);
 }
 
 // min_len: shortest code length of the book.  A segment holds at most
 // ceil(128 / min_len) codeword starts; the stage is sized for that.
-int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, void* stream) {
+int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, int ctas_per_sm,
+                  void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const uint32_t max_sym = (128 + min_len - 1) / (min_len ? min_len : 1);
-    return complete ? launch_decode_c<true>(a, t, max_sym, st) : launch_decode_c<false>(a, t, max_sym, st);
+    return complete ? launch_decode_c<true>(a, t, max_sym, ctas_per_sm, st)
+                    : launch_decode_c<false>(a, t, max_sym, ctas_per_sm, st);
 }
 
 }  // namespace hgap

@@ -128,6 +128,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     }
 }
 
+// The job owning global work item `it`: the largest j with item0s[j] <= it
+// (item0s ascends, item0s[count] is the total; empty jobs are skipped).
+__device__ __forceinline__ uint32_t find_job(const uint64_t* item0s, uint32_t count, uint64_t it) {
+    uint32_t lo = 0, hi = count;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (item0s[mid] <= it) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(kFull, v, d);
@@ -182,14 +194,17 @@ __device__ __forceinline__ uint64_t lookback_warp(uint64_t* rec, uint64_t tile, 
 // Publishing the aggregate and resolving the prefix are separate steps, so a
 // CTA can publish a tile's aggregate, decode its next tile, and resolve the
 // first tile afterwards, when its predecessors have long been published.
-__device__ __forceinline__ void lookback_publish(uint64_t* rec, uint64_t tile, uint64_t agg) {
-    st_relaxed_u64(rec + tile, (tile == 0 ? kFlagP : kFlagA) | (agg & kValueMask));
+// `first`: the tile starts its own scan (tile 0, or a batched job's first
+// tile); it publishes its inclusive prefix at once and resolves to 0, so no
+// look-back ever crosses into another job's tiles.
+__device__ __forceinline__ void lookback_publish(uint64_t* rec, uint64_t tile, uint64_t agg, bool first) {
+    st_relaxed_u64(rec + tile, (first ? kFlagP : kFlagA) | (agg & kValueMask));
 }
 
 template <int K>
-__device__ __forceinline__ uint64_t lookback_resolve(uint64_t* rec, uint64_t tile, uint64_t agg,
+__device__ __forceinline__ uint64_t lookback_resolve(uint64_t* rec, uint64_t tile, uint64_t agg, bool first,
                                                      uint32_t* status, uint32_t lane) {
-    if (tile == 0) return 0;
+    if (first) return 0;
     uint64_t excl = 0;
     int64_t top = (int64_t)tile - 1;
     for (;;) {

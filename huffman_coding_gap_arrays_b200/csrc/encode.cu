@@ -3,8 +3,10 @@
 // Replaces cuencoder + cu_get_gaparray (encoder/src/encoder.cu:142-379) and
 // produces the same bitstream and gap array bit for bit.
 //
-// Work unit: a super-tile of st_chunks x 8 KiB input bytes, taken by dynamic
-// id by persistent CTAs of 512 threads.  Its bit count is one dot product of
+// Work unit: a region (super-tile) of st_chunks x 8 KiB input bytes of one
+// job, taken by global id by persistent CTAs of 512 threads; the single-buffer
+// entry points run one job, the batched ones thousands, each with its own
+// codebook (the CTA reloads its code tables when the job changes).  Its bit count is one dot product of
 // its histogram (recorded by hist_st_kernel in the same pass that builds the
 // global histogram) with the code lengths, so a single bounded look-back over
 // super-tiles gives its first output bit G; no per-chunk look-back and no
@@ -59,74 +61,105 @@ constexpr size_t kEncSmem =
 
 struct EncShared {
     uint64_t mbar[kRing];       // one per ring buffer: its bulk copy landed
-    uint64_t G;                 // first output bit of the current super-tile
-    uint64_t cur;               // super-tile being encoded
-    uint64_t agg_cur;           // its bit count
+    EncJob job[2];              // slots: the current region's job and the next claimed one's
+    uint64_t item[2];           // their global region ids (>= nitems: none)
+    uint64_t agg[2];            // their bit counts
+    uint32_t job_id[2];
+    uint64_t G;                 // first output bit of the current region
     uint32_t warp_tot[kEncWarps];
     uint32_t carry;             // partial output word carried into the next chunk
     uint32_t gcarry[2];         // partial gap word carried, by chunk parity
+    uint64_t nitems;            // regions of the launch
+    uint32_t lut_job;           // job whose code tables are in the LUTs
     uint32_t abort;
+    uint32_t p_issued;          // producer: copies issued so far (chunk sequence number)
+    uint32_t p_chunk;           // producer: chunk index of the next copy within its region
+    int p_which;                // producer: next copy from the current region (0) or the next one (1)
 };
 
-// Warp 0: claims a super-tile and publishes its bit count right away, so that
-// no later super-tile's look-back waits on it.
-__device__ __forceinline__ void claim_super_tile(const EncArgs& a, const uint32_t* lutl, uint32_t lane,
-                                                 uint64_t& st, uint64_t& agg) {
-    uint32_t s = 0;
-    if (lane == 0) s = atomicAdd(a.counter, 1u);
-    st = __shfl_sync(kFull, s, 0);
-    agg = 0;
-    if (st < a.nst) {
+// Length and left-aligned code of `byte` from a job's table in global memory.
+__device__ __forceinline__ void code_of(const EncTable* t, uint32_t byte, uint32_t& c, uint32_t& len) {
+    const uint32_t e = t->e[byte];
+    len = (e >> 16) & 31u;
+    c = len ? (e & 0xffffu) << (32 - len) : 0u;
+}
+
+// Warp 0: claims a region into `slot`, copies its job there and publishes
+// its bit count at once, so that no later region's look-back waits on it.
+__device__ __forceinline__ void claim_region(const EncArgs& a, const uint32_t* lutl, EncShared& sh, int slot,
+                                             uint32_t lane) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(a.counter, 1u);
+    const uint64_t item = __shfl_sync(kFull, c, 0);
+    uint32_t job = 0;
+    uint64_t agg = 0;
+    __syncwarp();  // every lane is done reading the slot
+    if (item < sh.nitems) {
+        if (a.jobs) job = find_job(a.item0s, a.count, item);
+        const EncJob* src = a.jobs ? a.jobs + job : &a.single;
+        static_assert(sizeof(EncJob) % 8 == 0 && sizeof(EncJob) <= 256, "job copied as u64 lanes");
+        if (lane < sizeof(EncJob) / 8)
+            reinterpret_cast<uint64_t*>(&sh.job[slot])[lane] = reinterpret_cast<const uint64_t*>(src)[lane];
         uint64_t part = 0;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const uint32_t b = lane + 32 * j;
-            part += (uint64_t)a.st_hist[st * 256 + b] * (lutl[b << 5] & 31u);
+            const uint32_t len = a.jobs ? ((a.tables[job].e[b] >> 16) & 31u) : (lutl[b << 5] & 31u);
+            part += (uint64_t)a.st_hist[item * 256 + b] * len;
         }
         agg = warp_sum_u64(part);
-        if (lane == 0) lookback_publish(a.st_rec, st, agg);
+        if (lane == 0) lookback_publish(a.st_rec, item, agg, item == src->item0);
     }
+    if (lane == 0) {
+        sh.item[slot] = item;
+        sh.agg[slot] = agg;
+        sh.job_id[slot] = job;
+    }
+    __syncwarp();
 }
 
-__device__ __forceinline__ uint32_t st_chunks(const EncArgs& a, uint64_t st) {
-    const uint64_t v0 = st * (uint64_t)a.st_bytes;
-    const uint64_t v1 = (v0 + a.st_bytes < a.hi) ? v0 + a.st_bytes : a.hi;
+__device__ __forceinline__ uint32_t st_chunks(const EncJob& J, uint64_t st) {
+    const uint64_t v0 = st * (uint64_t)J.st_bytes;
+    const uint64_t v1 = (v0 + J.st_bytes < J.hi) ? v0 + J.st_bytes : J.hi;
     return (uint32_t)((v1 - v0 + kEncChunkBytes - 1) / kEncChunkBytes);
 }
 
 // Thread 0's bulk-copy producer.  Copies go out in the order the CTA encodes
-// chunks: the rest of the current super-tile, then the claimed next one; at
-// most kRing beyond the last chunk whose buffer is free again.
-struct Producer {
-    uint32_t issued = 0;  // copies issued so far (chunk sequence number)
-    uint64_t pst = ~0ull; // super-tile of the next copy
-    uint32_t pc = 0;      // its chunk index
-
-    __device__ __forceinline__ void run(const EncArgs& a, uint8_t* ring, EncShared& sh, uint32_t freed,
-                                        uint64_t cur, uint64_t nxt) {
-        while (issued < freed + kRing) {
-            if (pst >= a.nst) break;
-            if (pc >= st_chunks(a, pst)) {
-                if (pst == cur && nxt < a.nst) {
-                    pst = nxt;
-                    pc = 0;
-                    continue;
-                }
-                break;  // wait for the next claim
+// chunks: the rest of the current region, then the claimed next one; at most
+// kRing beyond the last chunk whose buffer is free again.  Its state lives in
+// shared memory (only thread 0 touches it), sparing every thread the registers.
+__device__ __forceinline__ void produce(const EncArgs& a, uint8_t* ring, EncShared& sh, uint32_t freed, int cur_slot) {
+    uint32_t issued = sh.p_issued, pc = sh.p_chunk;
+    int which = sh.p_which;
+    while (issued < freed + kRing) {
+        const int slot = cur_slot ^ which;
+        const uint64_t item = sh.item[slot];
+        if (item >= sh.nitems) break;
+        const EncJob& J = sh.job[slot];
+        const uint64_t st = item - J.item0;
+        if (pc >= st_chunks(J, st)) {
+            if (which == 0) {
+                which = 1;
+                pc = 0;
+                continue;
             }
-            const uint64_t v = pst * (uint64_t)a.st_bytes + (uint64_t)pc * kEncChunkBytes;
-            const uint64_t rem = ((a.hi + 15) & ~15ull) - v;  // through the end of the last 16-byte group
-            const uint32_t bytes = rem >= (uint64_t)kEncChunkBytes ? (uint32_t)kEncChunkBytes : (uint32_t)rem;
-            const uint32_t s = issued % kRing;
-            bulk_load(ring + (size_t)s * kEncChunkBytes, a.in_aligned + v, bytes, &sh.mbar[s]);
-            ++issued;
-            ++pc;
+            break;  // wait for the next claim
         }
+        const uint64_t v = st * (uint64_t)J.st_bytes + (uint64_t)pc * kEncChunkBytes;
+        const uint64_t rem = ((J.hi + 15) & ~15ull) - v;  // through the end of the last 16-byte group
+        const uint32_t bytes = rem >= (uint64_t)kEncChunkBytes ? (uint32_t)kEncChunkBytes : (uint32_t)rem;
+        const uint32_t s = issued % kRing;
+        bulk_load(ring + (size_t)s * kEncChunkBytes, J.in_aligned + v, bytes, &sh.mbar[s]);
+        ++issued;
+        ++pc;
     }
-};
+    sh.p_issued = issued;
+    sh.p_chunk = pc;
+    sh.p_which = which;
+}
 
 __global__ void __launch_bounds__(kEncThreads, 2)
-    encode_kernel(const EncArgs a, const __grid_constant__ EncTable tab) {
+    encode_kernel(const __grid_constant__ EncArgs a, const __grid_constant__ EncTable tab) {
     extern __shared__ __align__(16) uint32_t smem[];
     uint32_t* lutc = smem;                // [byte][lane]: code << (32 - len)
     uint32_t* lutl = smem + kLutWords;    // [byte][lane]: len (0x200 if absent)
@@ -136,113 +169,121 @@ __global__ void __launch_bounds__(kEncThreads, 2)
     __shared__ EncShared sh;
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < kLutWords; i += kEncThreads) {
-        const uint32_t e = tab.e[i >> 5];
-        const uint32_t l = (e >> 16) & 31u;
-        lutc[i] = l ? (e & 0xffffu) << (32 - l) : 0u;
-        lutl[i] = (e == kEncAbsent) ? 0x200u : l;
-    }
+    auto load_luts = [&](const EncTable& t) {
+        for (int i = tid; i < kLutWords; i += kEncThreads) {
+            const uint32_t e = t.e[i >> 5];
+            const uint32_t l = (e >> 16) & 31u;
+            lutc[i] = l ? (e & 0xffffu) << (32 - l) : 0u;
+            lutl[i] = (e == kEncAbsent) ? 0x200u : l;
+        }
+    };
+    if (!a.jobs) load_luts(tab);
     for (int i = tid; i < kImgWords; i += kEncThreads) img[i] = 0;
     if (tid == 0) {
-        // the histograms in the workspace must come from this very input
-        sh.abort = (a.tag[0] != a.hi - a.lo ||
-                    a.tag[1] != reinterpret_cast<uint64_t>(a.in_aligned) + a.lo);
+        // single path: the histograms in the workspace must come from this very input
+        sh.abort = a.tag && (a.tag[0] != a.single.hi - a.single.lo ||
+                             a.tag[1] != reinterpret_cast<uint64_t>(a.single.in_aligned) + a.single.lo);
         if (sh.abort) atomicOr(a.status, kDevPlan);
+        sh.lut_job = a.jobs ? ~0u : 0u;
+        sh.nitems = a.nitems_dev ? *a.nitems_dev : a.nitems;
+        sh.p_issued = 0;
+        sh.p_chunk = 0;
+        sh.p_which = 0;
         for (int s = 0; s < kRing; ++s) mbar_init(&sh.mbar[s], 1);
         mbar_init_fence();
     }
     __syncthreads();
     if (sh.abort) return;
-    const bool vec_ok = a.bits_aligned16 != 0;
 
-    Producer prod;                  // used by thread 0 only
-    uint64_t cur = 0, nxt = ~0ull;  // warp 0: super-tile being encoded, the one claimed next
-    uint64_t agg_cur = 0, agg_nxt = 0;
-    if (warp == 0) {
-        claim_super_tile(a, lutl, lane, cur, agg_cur);
-        if (cur < a.nst) claim_super_tile(a, lutl, lane, nxt, agg_nxt);
-        if (lane == 0) {
-            prod.pst = cur;
-            prod.run(a, ring, sh, 0, cur, nxt);
-        }
-    }
+    int cur_slot = 0;   // slot of the current region; the next one is in cur_slot ^ 1
     uint32_t cons = 0;  // chunks consumed so far (the ring's sequence number)
+    if (warp == 0) {
+        claim_region(a, lutl, sh, 0, lane);
+        if (sh.item[0] < sh.nitems) claim_region(a, lutl, sh, 1, lane);
+        else if (lane == 0) sh.item[1] = ~0ull;
+        if (lane == 0) produce(a, ring, sh, 0, 0);
+    }
+    __syncthreads();
 
     for (;;) {
-        // ---- warp 0: G of the current super-tile, bits before G -------------
+        const uint64_t item = sh.item[cur_slot];
+        if (item >= sh.nitems) break;
+        const EncJob& J = sh.job[cur_slot];
+        const uint32_t jid = sh.job_id[cur_slot];
+        const uint64_t st = item - J.item0;  // region within the job
+
+        // ---- warp 0: G of the current region, bits before G ---------------------
         if (warp == 0) {
-            uint64_t G = 0;
+            const uint64_t G = lookback_resolve<4>(a.st_rec, item, sh.agg[cur_slot], st == 0, a.status, lane);
             uint32_t head = 0, gcarry = 0;
-            if (cur < a.nst) {
-                G = lookback_resolve<4>(a.st_rec, cur, agg_cur, a.status, lane);
-                const uint32_t r = (uint32_t)(G & 31);
-                const uint32_t nibs = (uint32_t)((G >> 7) & 7);
-                if (G > 0 && (r != 0 || nibs != 0)) {
-                    // walk the previous super-tile's codes backwards from G
-                    const uint64_t wstart = G - r;
-                    const uint64_t gs = (G >> 10) << 10;
-                    // codes starting at or below `stop` can no longer reach the head
-                    // word (bits >= wstart) nor cross a boundary >= gs + 128
-                    uint64_t stop = r ? wstart : ~0ull;
-                    if (nibs && gs + 127 < stop) stop = gs + 127;
-                    uint64_t end = G;
-                    const uint64_t vfirst = cur * (uint64_t)a.st_bytes;  // first byte of this super-tile
-                    for (uint64_t base = 0;; base += 32) {
-                        const uint64_t v = vfirst - 1 - base - lane;     // may wrap below lo: no byte
-                        uint32_t c = 0, len = 0;
-                        if (vfirst >= base + lane + 1 && v >= a.lo) {
-                            const uint32_t byte = __ldg(a.in_aligned + v);
+            const uint32_t r = (uint32_t)(G & 31);
+            const uint32_t nibs = (uint32_t)((G >> 7) & 7);
+            if (G > 0 && (r != 0 || nibs != 0)) {
+                // walk the previous region's codes backwards from G
+                const uint64_t wstart = G - r;
+                const uint64_t gs = (G >> 10) << 10;
+                // codes starting at or below `stop` can no longer reach the head
+                // word (bits >= wstart) nor cross a boundary >= gs + 128
+                uint64_t stop = r ? wstart : ~0ull;
+                if (nibs && gs + 127 < stop) stop = gs + 127;
+                uint64_t end = G;
+                const uint64_t vfirst = st * (uint64_t)J.st_bytes;  // first byte of this region
+                for (uint64_t base = 0;; base += 32) {
+                    const uint64_t v = vfirst - 1 - base - lane;     // may wrap below lo: no byte
+                    uint32_t c = 0, len = 0;
+                    if (vfirst >= base + lane + 1 && v >= J.lo) {
+                        const uint32_t byte = __ldg(J.in_aligned + v);
+                        if (a.jobs) {
+                            code_of(a.tables + jid, byte, c, len);
+                        } else {
                             c = lutc[(byte << 5) | lane];
                             len = lutl[(byte << 5) | lane] & 31u;
                         }
-                        const uint32_t incl = warp_incl_scan(len, lane);
-                        const uint64_t ce = end - (incl - len);  // this code's end bit
-                        const uint64_t cs = ce - len;            // and start bit
-                        if (len) {
-                            if (r && ce > wstart)  // the code's right-aligned value, placed to end at ce
-                                head |= (uint32_t)(((uint64_t)(c >> (32 - len))) << (wstart + 32 - ce));
-                            const uint64_t b = (ce >> 7) << 7;   // last segment boundary <= end
-                            if (nibs && b > cs && b >= gs + 128)
-                                gcarry |= (uint32_t)(ce - b) << (4 * (uint32_t)(((b >> 7) - 1) & 7));
-                        }
-                        const uint32_t total = __shfl_sync(kFull, incl, 31);
-                        const uint64_t smin = end - total;  // start of the batch's last code
-                        end = smin;
-                        if (smin <= stop || total == 0) break;
                     }
-                    head = __reduce_or_sync(kFull, head);
-                    gcarry = __reduce_or_sync(kFull, gcarry);
+                    const uint32_t incl = warp_incl_scan(len, lane);
+                    const uint64_t ce = end - (incl - len);  // this code's end bit
+                    const uint64_t cs = ce - len;            // and start bit
+                    if (len) {
+                        if (r && ce > wstart)  // the code's right-aligned value, placed to end at ce
+                            head |= (uint32_t)(((uint64_t)(c >> (32 - len))) << (wstart + 32 - ce));
+                        const uint64_t b = (ce >> 7) << 7;   // last segment boundary <= end
+                        if (nibs && b > cs && b >= gs + 128)
+                            gcarry |= (uint32_t)(ce - b) << (4 * (uint32_t)(((b >> 7) - 1) & 7));
+                    }
+                    const uint32_t total = __shfl_sync(kFull, incl, 31);
+                    const uint64_t smin = end - total;  // start of the batch's last code
+                    end = smin;
+                    if (smin <= stop || total == 0) break;
                 }
+                head = __reduce_or_sync(kFull, head);
+                gcarry = __reduce_or_sync(kFull, gcarry);
             }
             if (lane == 0) {
-                sh.cur = cur;
-                sh.agg_cur = agg_cur;
                 sh.G = G;
                 sh.carry = head;  // 0 unless G % 32 != 0
                 sh.gcarry[cons & 1] = gcarry;
             }
         }
+        // batched: the job's code tables into the LUTs (the previous region is done with them)
+        if (a.jobs && jid != sh.lut_job) load_luts(a.tables[jid]);
         __syncthreads();
-        const uint64_t st = sh.cur;
-        if (st >= a.nst) break;
+        if (tid == 0) sh.lut_job = jid;
         uint64_t P = sh.G;
-        const uint64_t P_st = P;
 
-        // ---- stream the chunks ----------------------------------------------
-        const uint64_t v_st = st * (uint64_t)a.st_bytes;
-        const uint32_t nchunks = st_chunks(a, st);
+        // ---- stream the chunks --------------------------------------------------
+        const uint32_t nchunks = st_chunks(J, st);
+        uint64_t v0 = st * (uint64_t)J.st_bytes + (uint64_t)tid * kEncBpt;  // this thread's first byte
         bool overflow = false;
-        for (uint32_t c = 0; c < nchunks; ++c, ++cons) {
+        for (uint32_t c = 0; c < nchunks; ++c, ++cons, v0 += kEncChunkBytes) {
             const uint32_t stage = cons % kRing;
             mbar_wait(&sh.mbar[stage], (cons / kRing) & 1, a.status, true);
             const uint4 q = *reinterpret_cast<const uint4*>(ring + (size_t)stage * kEncChunkBytes + tid * 16);
 
             // lookups: left-aligned code and length per byte, bit count per thread
-            const uint64_t v0 = v_st + (uint64_t)c * kEncChunkBytes + (uint64_t)tid * kEncBpt;
             const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
             uint32_t cc[kEncBpt], ll[kEncBpt];
             uint32_t nbits = 0;
-            if (v0 >= a.lo && v0 + kEncBpt <= a.hi) {
+            if (v0 >= J.lo && v0 + kEncBpt <= J.hi) {
 #pragma unroll
                 for (int k = 0; k < kEncBpt; ++k) {
                     const uint32_t w = w4[k >> 2];
@@ -256,7 +297,7 @@ __global__ void __launch_bounds__(kEncThreads, 2)
 #pragma unroll
                 for (int k = 0; k < kEncBpt; ++k) {
                     const uint32_t idx = (((w4[k >> 2] >> (8 * (k & 3))) & 0xffu) << 5) | lane;
-                    const bool in = v0 + k >= a.lo && v0 + k < a.hi;
+                    const bool in = v0 + k >= J.lo && v0 + k < J.hi;
                     cc[k] = in ? lutc[idx] : 0u;
                     ll[k] = in ? lutl[idx] : 0u;
                     nbits += ll[k];
@@ -275,7 +316,7 @@ __global__ void __launch_bounds__(kEncThreads, 2)
                 // the word carried in (previous chunk's tail, or the rebuilt head word)
                 if (sh.carry) atomicOr(img + ((P >> 5) & 3), sh.carry);
                 fence_proxy_async_smem();
-                prod.run(a, ring, sh, cons + 1, cur, nxt);
+                produce(a, ring, sh, cons + 1, cur_slot);
             }
             uint32_t wt = lane < (uint32_t)kEncWarps ? sh.warp_tot[lane] : 0u;
             wt = warp_incl_scan(wt, lane);
@@ -318,18 +359,20 @@ __global__ void __launch_bounds__(kEncThreads, 2)
             const uint64_t E = P + L;
             const uint32_t j0 = (uint32_t)((P >> 5) - sb);
             const uint32_t j1 = (uint32_t)((E >> 5) - sb);
+            uint32_t* const bits = J.bits;
+            const uint64_t words = J.words;
             for (uint32_t g = tid; g <= j1 / 4; g += kEncThreads) {
                 const uint32_t j = 4 * g;
                 const uint4 wv = *reinterpret_cast<const uint4*>(img + j);
                 const uint64_t w = sb + j;
-                if (vec_ok && j >= j0 && j + 4 <= j1 && w + 4 <= a.words) {
-                    *reinterpret_cast<uint4*>(a.bits + w) = wv;
+                if (J.bits_aligned16 && j >= j0 && j + 4 <= j1 && w + 4 <= words) {
+                    *reinterpret_cast<uint4*>(bits + w) = wv;
                 } else {
                     const uint32_t wa[4] = {wv.x, wv.y, wv.z, wv.w};
 #pragma unroll
                     for (uint32_t k = 0; k < 4; ++k) {
                         if (j + k < j0 || j + k >= j1) continue;
-                        if (w + k < a.words) a.bits[w + k] = wa[k];
+                        if (w + k < words) bits[w + k] = wa[k];
                         else overflow = true;
                     }
                     if (j1 - j < 4) {
@@ -349,7 +392,7 @@ __global__ void __launch_bounds__(kEncThreads, 2)
                 for (uint64_t k = k0; k < k1; ++k)  // entry k = spill of global word 4k+3
                     v |= (uint32_t)spills[(uint32_t)(4 * k + 3 - sb)] << (4 * (uint32_t)(k & 7));
                 if (g < gwe) {
-                    if (g < a.gap_words) a.gaps[g] = v;
+                    if (g < J.gap_words) J.gaps[g] = v;
                     else overflow = true;
                 } else {
                     sh.gcarry[(cons + 1) & 1] = v;
@@ -360,36 +403,44 @@ __global__ void __launch_bounds__(kEncThreads, 2)
         if (overflow) atomicOr(a.status, kDevSize);
         __syncthreads();  // carries visible; the image is clear again
 
-        // ---- end of the super-tile ------------------------------------------
+        // ---- end of the region --------------------------------------------------
         if (tid == 0) {
-            if (P - P_st != sh.agg_cur) atomicOr(a.status, kDevPlan);  // histograms were not this input's
-            if (st + 1 == a.nst) {
-                if ((P & 31) && (P >> 5) < a.words) a.bits[P >> 5] = sh.carry;
+            if (P - sh.G != sh.agg[cur_slot]) atomicOr(a.status, kDevPlan);  // histograms were not this input's
+            if (sh.item[cur_slot] - J.item0 + 1 == J.nst) {
+                if ((P & 31) && (P >> 5) < J.words) J.bits[P >> 5] = sh.carry;
                 const uint64_t gwe = (P >> 7) >> 3;
-                if (gwe < a.gap_words) a.gaps[gwe] = sh.gcarry[cons & 1];
-                if ((P + 31) / 32 != a.words || (P + 127) / 128 != a.segments) atomicOr(a.status, kDevSize);
+                if (gwe < J.gap_words) J.gaps[gwe] = sh.gcarry[cons & 1];
+                if ((P + 31) / 32 != J.words || (P + 127) / 128 != J.segments) atomicOr(a.status, kDevSize);
             }
         }
         if (warp == 0) {
-            cur = nxt;
-            agg_cur = agg_nxt;
-            if (cur < a.nst) claim_super_tile(a, lutl, lane, nxt, agg_nxt);
-            if (lane == 0) prod.run(a, ring, sh, cons, cur, nxt);
+            // the next region becomes current; claim the one after it into the freed slot
+            const int old = cur_slot;
+            if (sh.item[old ^ 1] < sh.nitems) claim_region(a, lutl, sh, old, lane);
+            else if (lane == 0) sh.item[old] = ~0ull;
+            if (lane == 0) {
+                // the producer's cursor follows its region into the current slot
+                if (sh.p_which == 1) sh.p_which = 0;
+                else sh.p_chunk = 0;
+                produce(a, ring, sh, cons, old ^ 1);
+            }
         }
+        cur_slot ^= 1;
     }
 
     // every copy issued has been consumed, unless a wait gave up: never leave
     // the CTA with a copy still in flight into its shared memory
     if (tid == 0) {
-        const uint32_t first = prod.issued > (uint32_t)kRing ? prod.issued - kRing : 0u;
-        for (uint32_t i = first; i < prod.issued; ++i)
+        const uint32_t issued = sh.p_issued;
+        const uint32_t first = issued > (uint32_t)kRing ? issued - kRing : 0u;
+        for (uint32_t i = first; i < issued; ++i)
             mbar_wait(&sh.mbar[i % kRing], (i / kRing) & 1, a.status, false);
     }
 }
 
 // ------------------------------------------------------------- launchers ---
 
-int launch_encode(const EncArgs& a, const EncTable& t, void* stream) {
+int launch_encode(const EncArgs& a, const EncTable& t, int ctas_per_sm, void* stream) {
     static int sms = 0, per_sm = 0;
     if (sms == 0) {
         int dev = 0;
@@ -401,8 +452,9 @@ int launch_encode(const EncArgs& a, const EncTable& t, void* stream) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, encode_kernel, kEncThreads, kEncSmem);
         if (per_sm < 1) per_sm = 1;
     }
-    const uint64_t cap = (uint64_t)sms * per_sm;
-    const unsigned grid = (unsigned)(a.nst < cap ? a.nst : cap);
+    const int k = (ctas_per_sm > 0 && ctas_per_sm < per_sm) ? ctas_per_sm : per_sm;
+    const uint64_t cap = (uint64_t)sms * k;
+    const unsigned grid = (unsigned)(a.nitems_dev ? cap : (a.nitems < cap ? (a.nitems ? a.nitems : 1) : cap));
     encode_kernel<<<grid, kEncThreads, kEncSmem, static_cast<cudaStream_t>(stream)>>>(a, t);
     return cudaGetLastError();
 }

@@ -72,7 +72,11 @@ inline uint64_t encode_super_tiles(uint64_t lo_plus_n, uint64_t n) {
     return (lo_plus_n + st - 1) / st;
 }
 
-struct EncArgs {
+// One buffer to encode.  The single-buffer entry points pass one job by value;
+// the batched ones keep an array of them in the workspace.  Regions (units of
+// st_bytes input bytes) are numbered globally over the jobs of a launch: job
+// j owns regions [item0, item0 + nst).
+struct EncJob {
     const uint8_t* in_aligned;  // input rounded down to 16 bytes
     uint64_t lo;                // virtual index of the first input byte (in & 15)
     uint64_t hi;                // lo + n
@@ -81,24 +85,37 @@ struct EncArgs {
     uint32_t* gaps;
     uint64_t gap_words;
     uint64_t segments;
-    uint64_t* st_rec;          // [nst] look-back records over super-tiles
-    const uint32_t* st_hist;   // [nst][256] per-super-tile histograms
-    const uint64_t* tag;       // {n, input address} written by the histogram pass
+    uint64_t item0;             // global index of the job's first region
+    uint64_t nst;               // its regions
+    uint32_t st_bytes;          // region size in input bytes (a multiple of kEncChunkBytes)
+    uint32_t bits_aligned16;    // bits is 16-byte aligned: vector stores allowed
+};
+
+struct EncArgs {
+    EncJob single;              // the job, when jobs == nullptr
+    const EncJob* jobs;         // batched: [count]
+    const uint64_t* item0s;     // batched: [count + 1], item0 of each job and the total
+    const EncTable* tables;     // batched: [count]
+    uint32_t count;             // jobs (1 for the single-buffer path)
+    uint64_t nitems;            // regions over all jobs
+    const uint64_t* nitems_dev; // batched: the region count in device memory (overrides nitems)
+    uint64_t* st_rec;           // [nitems] look-back records over regions
+    const uint32_t* st_hist;    // [nitems][256] per-region histograms
+    const uint64_t* tag;        // single path: {n, input address} written by the histogram pass
     uint32_t* counter;
     uint32_t* status;
-    uint64_t nst;
-    uint32_t st_bytes;         // super-tile size in input bytes
-    uint32_t bits_aligned16;   // d_bits is 16-byte aligned: vector stores allowed
 };
 
 struct HistStArgs {
-    const uint8_t* in_aligned;
-    uint64_t lo, hi;
-    uint32_t* hist;      // [256] global histogram (zeroed by the launcher)
-    uint32_t* st_hist;   // [nst][256]
-    uint64_t* tag;       // receives {n, input address}
-    uint64_t nst;
-    uint32_t st_bytes;
+    EncJob single;
+    const EncJob* jobs;
+    const uint64_t* item0s;
+    uint32_t count;
+    uint64_t nitems;
+    const uint64_t* nitems_dev; // batched: the region count in device memory (overrides nitems)
+    uint32_t* hist;             // [count][256] histograms (zeroed before the launch)
+    uint32_t* st_hist;          // [nitems][256]
+    uint64_t* tag;              // single path: receives {n, input address}
 };
 
 // ---------------------------------------------------------------- decoder ---
@@ -114,27 +131,42 @@ struct DecTable {
     uint16_t t2[kDecT2Cap];
 };
 
-struct DecArgs {
+// One stream to decode (same single / batched scheme as EncJob).  Its tiles
+// use look-back records [item0, item0 + ntiles).
+struct DecJob {
     const uint32_t* bits;
     uint64_t words;
     const uint32_t* gaps;
-    uint64_t segments;
     uint64_t gap_words;
+    uint64_t segments;
     uint8_t* out_aligned;  // output rounded down to 16 bytes
     uint64_t out_lo;       // out & 15
     uint64_t n;
+    uint64_t item0;        // first look-back record of the job
+    uint64_t ntiles;
+};
+
+struct DecArgs {
+    DecJob single;              // the job, when jobs == nullptr
+    const DecJob* jobs;         // batched: [count]
+    const uint32_t* job_of;     // batched: [nitems] job of each tile of this launch
+    const uint64_t* item0s;     // batched: [count] first tile of each job in this launch's numbering
+    const DecTable* tables;     // batched: [count]
+    uint32_t count;
+    uint64_t nitems;            // tiles in this launch
+    const uint64_t* nitems_dev; // batched: the tile count in device memory (overrides nitems)
     uint64_t* lookback;
     uint32_t* counter;
     uint32_t* status;
-    uint64_t ntiles;
 };
 
 // --------------------------------------------------------------- launchers --
 // Implemented in the .cu files; return cudaError_t as int.
 int launch_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, void* stream);
-int launch_encode(const EncArgs& a, const EncTable& t, void* stream);
-int launch_hist_st(const HistStArgs& a, void* stream);
-int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, void* stream);
+int launch_encode(const EncArgs& a, const EncTable& t, int ctas_per_sm, void* stream);
+int launch_hist_st(const HistStArgs& a, int ctas_per_sm, void* stream);
+int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, int ctas_per_sm,
+                  void* stream);
 uint64_t decode_tiles(uint64_t segments);
 
 // ------------------------------------------------------------- host helpers -

@@ -76,39 +76,48 @@ __global__ void __launch_bounds__(kHistThreads, 4)
     }
 }
 
-// Histogram pass of the encoder: the same lane-replicated counters, with the
-// input cut into super-tiles (static round-robin over CTAs).  After each
-// super-tile the CTA folds its 32 copies and stores the difference to the
-// previous fold as that super-tile's histogram, so the encoder can compute
-// every super-tile's bit count without reading its bytes again.  The global
-// histogram is the sum of a CTA's final fold, added with one atomic per bin.
-__global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const HistStArgs a) {
+// Histogram pass of the encoder: the same lane-replicated counters, over the
+// regions of one or many jobs (a contiguous run of regions per CTA).  After
+// each region the CTA folds its 32 copies and stores the difference to the
+// previous fold as that region's histogram, so the encoder can compute every
+// region's bit count without reading its bytes again.  A job's histogram is
+// the sum of its regions', added with one atomic per bin whenever the CTA's
+// run leaves the job.
+__global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const __grid_constant__ HistStArgs a) {
     __shared__ uint32_t h[256 * 32];
     for (int i = threadIdx.x; i < 256 * 32; i += kHistThreads) h[i] = 0;
     __syncthreads();
     const uint32_t tid = threadIdx.x;
     uint32_t* hl = h + (tid & 31);
-    uint32_t prev = 0;  // running fold of bin `tid` (tid < 256)
-    for (uint64_t st = blockIdx.x; st < a.nst; st += gridDim.x) {
-        const uint64_t v0 = st * (uint64_t)a.st_bytes;
-        const uint64_t v1 = (v0 + a.st_bytes < a.hi) ? v0 + a.st_bytes : a.hi;
-        const uint64_t lo_v = v0 > a.lo ? v0 : a.lo;
+    uint32_t prev = 0, acc = 0;  // running fold of bin `tid` (tid < 256); the job's sum so far
+    const uint64_t nitems = a.nitems_dev ? *a.nitems_dev : a.nitems;
+    const uint64_t per = (nitems + gridDim.x - 1) / gridDim.x;
+    const uint64_t it0 = (uint64_t)blockIdx.x * per;
+    const uint64_t it1 = it0 + per < nitems ? it0 + per : nitems;
+    uint32_t job = 0;
+    for (uint64_t it = it0; it < it1; ++it) {
+        if (a.jobs && (it == it0 || it >= a.item0s[job + 1])) job = find_job(a.item0s, a.count, it);
+        const EncJob& J = a.jobs ? a.jobs[job] : a.single;
+        const uint64_t v0 = (it - J.item0) * (uint64_t)J.st_bytes;
+        const uint64_t v1 = (v0 + J.st_bytes < J.hi) ? v0 + J.st_bytes : J.hi;
+        const uint64_t lo_v = v0 > J.lo ? v0 : J.lo;
+        const uint8_t* in = J.in_aligned;
         const uint64_t c0 = (lo_v + 15) >> 4, c1 = v1 >> 4;  // chunks wholly inside
         uint64_t c = c0 + tid;
         for (; c + (kHistUnroll - 1) * kHistThreads < c1; c += kHistUnroll * kHistThreads) {
             uint4 v[kHistUnroll];
 #pragma unroll
-            for (int u = 0; u < kHistUnroll; ++u) v[u] = ld_stream_v4(a.in_aligned + ((c + u * kHistThreads) << 4));
+            for (int u = 0; u < kHistUnroll; ++u) v[u] = ld_stream_v4(in + ((c + u * kHistThreads) << 4));
 #pragma unroll
             for (int u = 0; u < kHistUnroll; ++u) hist_chunk(hl, v[u]);
         }
-        for (; c < c1; c += kHistThreads) hist_chunk(hl, ld_stream_v4(a.in_aligned + (c << 4)));
-        // ragged head chunk (first super-tile only) and tail chunk (last only)
+        for (; c < c1; c += kHistThreads) hist_chunk(hl, ld_stream_v4(in + (c << 4)));
+        // ragged head chunk (a job's first region only) and tail chunk (its last only)
         uint64_t q = ~0ull;
         if (tid == 0 && (lo_v & 15)) q = lo_v >> 4;
         if (tid == 1 && (v1 & 15) && (v1 >> 4) >= c0) q = v1 >> 4;
         if (q != ~0ull) {
-            const uint4 v = ld_stream_v4(a.in_aligned + (q << 4));
+            const uint4 v = ld_stream_v4(in + (q << 4));
             const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
             for (uint64_t b = q << 4; b < (q << 4) + 16; ++b) {
                 if (b < lo_v || b >= v1) continue;
@@ -116,26 +125,31 @@ __global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const HistStAr
             }
         }
         __syncthreads();
+        const bool leave = it + 1 == it1 || it + 1 == J.item0 + J.nst;
         if (tid < 256) {
             uint32_t s = 0;
 #pragma unroll 8
             for (int j = 0; j < 32; ++j) s += h[tid * 32 + ((j + tid) & 31)];
-            a.st_hist[st * 256 + tid] = s - prev;
+            const uint32_t d = s - prev;
+            a.st_hist[it * 256 + tid] = d;
             prev = s;
+            acc += d;
+            if (leave) {
+                if (acc) atomicAdd(a.hist + 256 * (uint64_t)job + tid, acc);
+                acc = 0;
+            }
         }
         __syncthreads();
     }
-    if (tid < 256 && prev) atomicAdd(a.hist + tid, prev);
-    if (blockIdx.x == 0 && tid == 0) {
-        a.tag[0] = a.hi - a.lo;
-        a.tag[1] = reinterpret_cast<uint64_t>(a.in_aligned) + a.lo;
+    if (a.tag && blockIdx.x == 0 && tid == 0) {
+        a.tag[0] = a.single.hi - a.single.lo;
+        a.tag[1] = reinterpret_cast<uint64_t>(a.single.in_aligned) + a.single.lo;
     }
 }
 
-int launch_hist_st(const HistStArgs& a, void* stream) {
+// `hist` must be zeroed by the caller ([count][256]).
+int launch_hist_st(const HistStArgs& a, int ctas_per_sm, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemsetAsync(a.hist, 0, 256 * sizeof(uint32_t), st);
-    if (e != cudaSuccess) return e;
     static int sms = 0, per_sm = 0;
     if (sms == 0) {
         int dev = 0;
@@ -144,8 +158,9 @@ int launch_hist_st(const HistStArgs& a, void* stream) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hist_st_kernel, kHistThreads, 0);
         if (per_sm < 1) per_sm = 1;
     }
-    const uint64_t cap = (uint64_t)sms * per_sm;
-    const unsigned grid = (unsigned)(a.nst < cap ? a.nst : cap);
+    const int k = (ctas_per_sm > 0 && ctas_per_sm < per_sm) ? ctas_per_sm : per_sm;
+    const uint64_t cap = (uint64_t)sms * k;
+    const unsigned grid = (unsigned)(a.nitems_dev ? cap : (a.nitems < cap ? (a.nitems ? a.nitems : 1) : cap));
     hist_st_kernel<<<grid, kHistThreads, 0, st>>>(a);
     return cudaGetLastError();
 }

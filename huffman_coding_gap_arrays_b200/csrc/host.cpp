@@ -215,6 +215,21 @@ hgap_status hgap_codebook_from_symbols(const hgap_symlen* symbols, uint32_t coun
     return assign_codes(cb);
 }
 
+hgap_status hgap_decode_table_build(const hgap_codebook* cb, uint16_t* t1, uint16_t* t2) {
+    if (!cb || !t1 || !t2) return HGAP_ERR_INVALID_ARG;
+    hgap_codebook book;
+    if (cb->symbol_count > 256) return HGAP_ERR_CORRUPT;
+    hgap_status st = hgap_codebook_from_symbols(cb->symbols, cb->symbol_count, &book);
+    if (st != HGAP_OK) return st;
+    if (book.symbol_count == 0) return HGAP_ERR_CORRUPT;
+    hgap::DecTable t;
+    st = hgap::make_dec_table(book, &t);
+    if (st != HGAP_OK) return st;
+    std::memcpy(t1, t.t1, sizeof(t.t1));
+    std::memcpy(t2, t.t2, sizeof(t.t2));
+    return HGAP_OK;
+}
+
 size_t hgap_container_bytes(uint32_t symbol_count, uint64_t words, uint64_t segments) {
     return 8 + 2 * (size_t)symbol_count + 12 + 4 * (size_t)((segments + 7) / 8) + 4 * (size_t)words;
 }

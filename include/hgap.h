@@ -179,6 +179,85 @@ hgap_status hgap_decode_noalloc(const uint32_t* d_bits, uint64_t words, const ui
                                 uint64_t segments, const hgap_codebook* cb, uint8_t* d_out,
                                 uint64_t n, hgap_stream_t stream);
 
+/* ---------------------------------------------------- codebooks on the device
+ * No counterpart in the reference (its device-side attempt,
+ * decoder/src/decoder.cu:36-88, is unfinished): the host builder
+ * hgap_codebook_build run on the GPU, one warp per book, with identical
+ * results (stable order by count, package-merge with the same tie rule,
+ * canonical codes).  d_hists: count x 256 counts; d_books: count codebooks;
+ * d_sizes: count sizes (may be NULL).  Stream-ordered, allocates nothing. */
+hgap_status hgap_codebook_build_device(uint32_t count, const uint32_t* d_hists, hgap_codebook* d_books,
+                                       hgap_sizes* d_sizes, hgap_stream_t stream);
+
+/* The decoder's two-level table (level 1: 2^11 u16 entries, level 2: 2560
+ * u16 entries) from a codebook, on the host and on the device (one warp per
+ * book).  Exposed so the two builders can be checked against each other. */
+#define HGAP_DEC_T1_ENTRIES 2048
+#define HGAP_DEC_T2_ENTRIES 2560
+hgap_status hgap_decode_table_build(const hgap_codebook* cb, uint16_t* t1, uint16_t* t2);
+hgap_status hgap_decode_table_build_device(uint32_t count, const hgap_codebook* d_books, uint16_t* d_tables,
+                                           uint32_t* d_status, hgap_stream_t stream);
+
+/* -------------------------------------------------------------- batched path
+ * No counterpart in the reference.  Thousands of independent buffers, each
+ * with its own codebook built on the device, compressed or decompressed by a
+ * fixed sequence of persistent launches that never returns to the host (so
+ * it can be captured in a CUDA graph).  Each buffer keeps the reference's
+ * format: the bitstream and gap array of buffer i are exactly what
+ * hgap_encode would write for it with the book hgap_codebook_build makes
+ * from its histogram.
+ *
+ * Outputs of hgap_batch_compress: the bitstreams, packed into one bits arena
+ * (each starting 16-byte aligned), the gap arrays packed into one gaps arena,
+ * and one hgap_batch_entry per buffer in device memory with its sizes,
+ * offsets and codebook (container order).  hgap_batch_decompress takes the
+ * same arenas and entries back. */
+typedef struct hgap_batch_entry {
+    uint64_t n;            /* uncompressed bytes */
+    uint64_t bits;         /* code bits */
+    uint64_t words;        /* W */
+    uint64_t segments;     /* S */
+    uint64_t gap_words;    /* ceil(S / 8) */
+    uint64_t bits_offset;  /* word offset of the bitstream in the bits arena */
+    uint64_t gaps_offset;  /* word offset of the gap array in the gaps arena */
+    uint32_t symbol_count;
+    uint32_t status;       /* 0, or an hgap_status for this buffer (e.g. arena too small) */
+    hgap_symlen symbols[256]; /* container order: most frequent first */
+} hgap_batch_entry;
+
+/* Launch shape; every choice leaves the output format unchanged. */
+typedef struct hgap_batch_config {
+    uint32_t region_chunks;    /* encoder region = region_chunks x 8 KiB (1..32; 0 = 8) */
+    uint32_t hist_ctas_per_sm; /* persistent grids, CTAs per SM (0 = occupancy maximum) */
+    uint32_t enc_ctas_per_sm;
+    uint32_t dec_ctas_per_sm;
+} hgap_batch_config;
+
+/* Worst-case sizes from the uncompressed sizes (host array). */
+size_t hgap_batch_compress_workspace_bytes(uint32_t count, const uint64_t* sizes,
+                                           const hgap_batch_config* cfg);
+size_t hgap_batch_decompress_workspace_bytes(uint32_t count, const uint64_t* sizes);
+uint64_t hgap_batch_bits_capacity(uint32_t count, const uint64_t* sizes);  /* words */
+uint64_t hgap_batch_gaps_capacity(uint32_t count, const uint64_t* sizes);  /* words */
+
+/* d_inputs / d_sizes: device arrays of count input pointers and sizes.
+ * d_region_chunks: optional device array of per-buffer region sizes (in 8 KiB
+ * chunks, raised to cfg->region_chunks at least); NULL = cfg for all.
+ * Workspace 16-byte aligned, from hgap_batch_compress_workspace_bytes with
+ * the same sizes and cfg. */
+hgap_status hgap_batch_compress(uint32_t count, const uint8_t* const* d_inputs, const uint64_t* d_sizes,
+                                const uint8_t* d_region_chunks, uint32_t* d_bits, uint64_t bits_capacity,
+                                uint32_t* d_gaps, uint64_t gaps_capacity, hgap_batch_entry* d_entries,
+                                void* d_workspace, size_t workspace_bytes, const hgap_batch_config* cfg,
+                                hgap_stream_t stream);
+/* d_outputs: device array of count output pointers (entry i's n bytes each). */
+hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entries, const uint32_t* d_bits,
+                                  const uint32_t* d_gaps, uint8_t* const* d_outputs, void* d_workspace,
+                                  size_t workspace_bytes, const hgap_batch_config* cfg, hgap_stream_t stream);
+/* Waits for `stream`; the device status of the last batched call that used
+ * this workspace, like hgap_workspace_status. */
+hgap_status hgap_batch_status(const void* d_workspace, hgap_stream_t stream);
+
 /* ------------------------------------------------------------------ container
  * Writer encoder/src/huff.cpp:111-125, reader decoder/src/huff.cpp:27-81:
  * u64 symbol_count; symbol_count x {u8 symbol, u8 length}; u32 n; u32 W;

@@ -138,3 +138,25 @@ def test_encoded_bits_is_64bit():
     h[:3] = [3_000_000_000, 2_900_000_000, 1_000_000_000]
     book, sizes = H.Codebook.from_histogram(h)
     assert sizes.bits == sum(int(book.length[b]) * int(h[b]) for b in range(3))
+
+
+def test_batch_host_queries():
+    """The batched path's host-side size queries (no GPU needed)."""
+    import ctypes as C
+    from huffman_coding_gap_arrays_b200._lib import BatchConfig, BatchEntry
+    L = _lib.lib()
+    assert C.sizeof(BatchEntry) == 576
+    sizes = np.array([0, 1, 4096, 8192 * 8 + 1, 1 << 22], np.uint64)
+    p = sizes.ctypes.data_as(C.POINTER(C.c_uint64))
+    cfg = BatchConfig(8, 0, 0, 0)
+    enc = L.hgap_batch_compress_workspace_bytes(sizes.size, p, C.byref(cfg))
+    dec = L.hgap_batch_decompress_workspace_bytes(sizes.size, p)
+    # regions: ceil((n + 15) / 64 KiB) per non-empty buffer
+    regions = sum(int(-(-(int(n) + 15) // 65536)) for n in sizes if n)
+    assert enc >= regions * (8 + 1024)
+    assert dec >= sum(int(-(-int(n) // 4096)) for n in sizes) * 40
+    cfg1 = BatchConfig(1, 0, 0, 0)
+    assert L.hgap_batch_compress_workspace_bytes(sizes.size, p, C.byref(cfg1)) > enc
+    # worst case 16 bits per byte, each bitstream rounded up to 16 bytes
+    assert L.hgap_batch_bits_capacity(sizes.size, p) == sum(((int(n) * 16 + 31) // 32 + 3) & ~3 for n in sizes)
+    assert L.hgap_batch_gaps_capacity(sizes.size, p) == sum(((int(n) * 16 + 127) // 128 + 7) // 8 for n in sizes)
