@@ -1,12 +1,20 @@
 #!/usr/bin/env python
 """Throughput of the Huffman-with-gap-arrays path on B200.
 
-One step = one full pass of the path over the workload buffer:
-histogram (GPU) -> codebook (host, from the 1 KiB histogram) -> fused encode
-(GPU) -> decode (GPU), i.e. the reference's bin/encoder followed by
-bin/decoder minus file I/O.  The default workload is the large single-buffer
-config: 1 GiB of 1 MiB blocks, each Zipf(1.05) or 8-bit quantised N(0,1),
-seeded (inputs > L2, so no flush is needed between steps).
+Default workload (`batch4096`): 4096 independent buffers, sizes log-uniform
+in [4 KiB, 4 MiB] (~2.46 GB), each Zipf(s ~ U[0.8,1.6]) or quantised
+Gaussian (sigma ~ U[0.5,4]) by its seed, each with its own codebook.  One
+step = compress every buffer (histograms -> codebooks on the device ->
+encode) then decompress every buffer, as two captured CUDA graphs of the
+batched path, with the launch configuration picked by the autotuner.  The
+plain single-buffer path, run buffer by buffer through the public API on the
+same buffers, is timed beside it (`plain`, `speedup_vs_plain`).
+
+Single-buffer workloads (`--workload mixed_1g | zipf_16m | mixed_256m`): one
+step = histogram (GPU) -> codebook (host, from the 1 KiB histogram) -> fused
+encode (GPU) -> decode (GPU), i.e. the reference's bin/encoder followed by
+bin/decoder minus file I/O.  All inputs exceed the 126 MB L2, so no flush is
+needed between steps.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
     torchrun --nproc-per-node N bench.py --gpus N ...   (N > 1: one replica per GPU)
@@ -34,6 +42,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "enc/dec GB/s of raw bytes, % HBM roofline; batched+tuned vs plain on 1 B200"
 WORKLOADS = {
+    "batch4096": ("4096 uint8 buffers, sizes log-uniform in [4 KiB, 4 MiB] (seed 4), each Zipf(s~U[0.8,1.6]) "
+                  "or clamp(round(128 + sigma z)) with sigma~U[0.5,4] by its seed, own codebook each", 0),
     "mixed_1g": ("1 GiB uint8, 1 MiB blocks of Zipf(1.05) or 8-bit quantised N(0,1) "
                  "(+-3 sigma -> 0..255), block kind by hash(seed, block), seed 2", 1 << 30),
     "zipf_16m": ("16 MiB uint8 i.i.d. Zipf(s=1.2) over 256 symbols, seed 1", 16 << 20),
@@ -47,7 +57,10 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="hgap", choices=["hgap", "reference"])
-    p.add_argument("--workload", default="mixed_1g", choices=sorted(WORKLOADS))
+    p.add_argument("--workload", default="batch4096", choices=sorted(WORKLOADS))
+    p.add_argument("--plain-buffers", type=int, default=4096,
+                   help="buffers of the batch timed through the plain per-buffer path")
+    p.add_argument("--no-tune", action="store_true", help="skip the autotuner: fixed default config")
     p.add_argument("--cpu-sample-mib", type=int, default=256)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -154,6 +167,44 @@ def make_workload(name: str, device, rank: int = 0):
     return WL.zipf_buffer(16 << 20, 1.2, seed=1 + 1000 * rank, device=device)
 
 
+def batch_workload(device, rank: int = 0):
+    """The 4096 buffers of the batched workload, packed back to back in one
+    device allocation (so the end-to-end copies are one H2D and one D2H)."""
+    import torch
+    from huffman_coding_gap_arrays_b200 import workloads as WL
+    sizes = WL.batch_sizes(4096, seed=4 + 1000 * rank)
+    total = sum(sizes)
+    flat = torch.empty(total, dtype=torch.uint8, device=device)
+    views, p = [], 0
+    for i, n in enumerate(sizes):
+        v = flat[p:p + n]
+        v.copy_(WL.batch_buffer(n, 1000 + i + 1000003 * rank, device=device))
+        views.append(v)
+        p += n
+    return sizes, flat, views
+
+
+def cpu_batch_sample(sizes, flat_host, threads: int, budget: int):
+    """Oracle round trips of the batch's first buffers up to `budget` bytes."""
+    from oracle import oracle as O
+    import numpy as np
+    t, done, p = 0.0, 0, 0
+    for n in sizes:
+        if done >= budget:
+            break
+        xs = np.ascontiguousarray(flat_host[p:p + n])
+        t0 = time.perf_counter()
+        h = O.histogram_mt(xs, threads)
+        cb = O.codebook(h)
+        bits, gaps = O.encode_mt(xs, cb, cb.total_bits, threads)
+        y = O.decode_mt(bits, gaps, (cb.total_bits + 127) // 128, cb, n, threads)
+        t += time.perf_counter() - t0
+        assert np.array_equal(y, xs)
+        done += n
+        p += n
+    return done, t
+
+
 def run_reference(args, rank: int, world: int):
     """`--impl reference`: the reference path's CPU implementation (the oracle
     port -- the reference itself has no CPU encoder/decoder) on the box's host
@@ -162,20 +213,39 @@ def run_reference(args, rank: int, world: int):
         return
     import numpy as np
     import torch
-    desc, n_full = WORKLOADS[args.workload]
-    x = make_workload(args.workload, "cpu")
-    sample = min(n_full, args.cpu_sample_mib << 20)
-    xs = np.ascontiguousarray(x[:sample].numpy())
     threads = host_threads()
-    for _ in range(args.warmup):
-        cpu_roundtrip(xs, threads)
-    times = []
-    for _ in range(args.steps):
-        dt, y = cpu_roundtrip(xs, threads)
-        times.append(dt)
-    assert np.array_equal(y, xs)
-    t = sum(times)
-    value = sample * args.steps / t / 1e9
+    if args.workload == "batch4096":
+        desc = WORKLOADS["batch4096"][0]
+        sizes, flat, _ = batch_workload("cpu")
+        fh = flat.numpy()
+        budget = args.cpu_sample_mib << 20
+        for _ in range(args.warmup):
+            cpu_batch_sample(sizes, fh, threads, budget // 8)
+        done, t = 0, 0.0
+        for _ in range(args.steps):
+            d, dt = cpu_batch_sample(sizes, fh, threads, budget)
+            done += d
+            t += dt
+        value = done / t / 1e9
+        n_full, sample = sum(sizes), done // max(args.steps, 1)
+        what = (f"the batch's first buffers up to {budget >> 20} MiB ({sample} bytes), per buffer "
+                f"histogram+codebook+encode+decode (oracle/hgap_oracle.c, pthreads)")
+    else:
+        desc, n_full = WORKLOADS[args.workload]
+        x = make_workload(args.workload, "cpu")
+        sample = min(n_full, args.cpu_sample_mib << 20)
+        xs = np.ascontiguousarray(x[:sample].numpy())
+        for _ in range(args.warmup):
+            cpu_roundtrip(xs, threads)
+        times = []
+        for _ in range(args.steps):
+            dt, y = cpu_roundtrip(xs, threads)
+            times.append(dt)
+        assert np.array_equal(y, xs)
+        t = sum(times)
+        value = sample * args.steps / t / 1e9
+        what = (f"first {sample >> 20} MiB of the workload, histogram+codebook+encode+decode per step "
+                f"(oracle/hgap_oracle.c, pthreads)")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GB/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -183,13 +253,218 @@ def run_reference(args, rank: int, world: int):
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": {"workload": desc, "bytes": n_full, "sample_bytes": sample},
         "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": f"first {sample >> 20} MiB of the workload, histogram+codebook+"
-                                   f"encode+decode per step (oracle/hgap_oracle.c, pthreads)"},
+                         "sample": what},
         "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     del torch
+
+
+def run_batch(args, rank, world, dev, pg):
+    """The batched path on the 4096-buffer workload (see the module docstring)."""
+    import numpy as np
+    import torch
+    import huffman_coding_gap_arrays_b200 as H
+    from huffman_coding_gap_arrays_b200 import batch as B
+    from huffman_coding_gap_arrays_b200 import tuner as T
+
+    desc = WORKLOADS["batch4096"][0]
+    sizes, flat, ins = batch_workload(dev, rank)
+    total = sum(sizes)
+    flat_out = torch.empty(total, dtype=torch.uint8, device=dev)
+    outs, p = [], 0
+    for n in sizes:
+        outs.append(flat_out[p:p + n])
+        p += n
+
+    # ---- tuning (untimed): exhaustive search of the launch space ------------
+    if args.no_tune:
+        cfg = B.LaunchConfig()
+        tuning = {"method": "fixed default", "config": vars(cfg)}
+    else:
+        t0 = time.time()
+        res = T.Autotuner(reps=2, warmup=1).tune(ins, outs)
+        cfg = res.config
+        tuning = {"method": "autotuner (exhaustive)", "config": vars(cfg),
+                  "candidates": len(T.compress_space()) + len(T.DEC_CTAS),
+                  "seconds": round(time.time() - t0, 2)}
+        torch.cuda.empty_cache()
+    plan = B.BatchCodec(sizes, cfg, device=dev)
+    plan.bind(ins, outs)
+    plan.compress()
+    plan.decompress()
+    plan.check()
+    if not torch.equal(flat_out, flat):
+        raise SystemExit("batched round trip mismatch")
+    ents = plan.entries_host()
+    C = sum(4 * (e.words + e.gap_words) for e in ents)
+    used_bits = max(e.bits_offset + e.words for e in ents)
+    used_gaps = max(e.gaps_offset + e.gap_words for e in ents)
+    g_c = plan.capture(compress=True, decompress=False)
+    g_d = plan.capture(compress=False, decompress=True)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        g_c.replay()
+        g_d.replay()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(dev.index or 0) if rank == 0 else None
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(args.steps):
+        evs[k][0].record(stream)
+        g_c.replay()
+        evs[k][1].record(stream)
+        g_d.replay()
+        evs[k][2].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clock_info = clocks.stop() if clocks else None
+    ms = t0.elapsed_time(t1)
+    plan.check()
+    if not torch.equal(flat_out, flat):
+        raise SystemExit("batched round trip mismatch after the timed steps")
+    if pg:
+        tm = torch.tensor([ms], device=dev)
+        pg.all_reduce(tm, op=pg.ReduceOp.MAX)
+        ms = float(tm.item())
+    c_ms = sum(e[0].elapsed_time(e[1]) for e in evs) / args.steps
+    d_ms = sum(e[1].elapsed_time(e[2]) for e in evs) / args.steps
+    peak, peak_src = peak_hbm()
+    alg = {"compress": 2 * total + C, "decompress": C + total}
+    ph_ms = {"compress": c_ms, "decompress": d_ms}
+    kernels = {k: {"ms": round(ph_ms[k], 4), "raw_gbs": round(total / ph_ms[k] / 1e6, 1),
+                   "alg_gbs": round(alg[k] / ph_ms[k] / 1e6, 1),
+                   "frac_of_" + peak_src: round(alg[k] / ph_ms[k] / 1e6 / peak, 4)} for k in ph_ms}
+    dom = max(ph_ms, key=ph_ms.get)
+    achieved = alg[dom] / ph_ms[dom] / 1e6
+    tr = traffic_ratios()
+    roofline = {"bound": "hbm", "kernel": "batched " + dom, "achieved": round(achieved, 1), "peak": peak,
+                "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": (round(tr["batch_" + dom] * total) if ("batch_" + dom) in tr else None),
+                "algorithmic_bytes": alg[dom]}
+
+    # ---- the plain single-buffer path, buffer by buffer, same buffers --------
+    plain = None
+    kp = min(args.plain_buffers, len(sizes))
+    if kp:
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        comp = [H.compress(x) for x in ins[:kp]]
+        torch.cuda.synchronize()
+        b_ = time.perf_counter()
+        dec_out = [H.decompress(c) for c in comp]
+        torch.cuda.synchronize()
+        c_ = time.perf_counter()
+        sub = sum(sizes[:kp])
+        if not all(torch.equal(y, x) for y, x in zip(dec_out, ins[:kp])):
+            raise SystemExit("plain round trip mismatch")
+        plain = {"buffers": kp, "bytes": sub, "compress_gbs": round(sub / (b_ - a) / 1e9, 3),
+                 "decompress_gbs": round(sub / (c_ - b_) / 1e9, 3),
+                 "roundtrip_gbs": round(sub / (c_ - a) / 1e9, 3),
+                 "how": "codec.compress / codec.decompress per buffer (histogram -> host codebook -> "
+                        "encode; decode), wall clock with device syncs"}
+        del comp, dec_out
+
+    # ---- end to end through the public API, host buffers ---------------------
+    e2e = None
+    if not args.no_e2e:
+        in_host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+        in_host.copy_(flat)
+        out_host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+        ent_host = torch.empty(plan.entries.numel(), dtype=torch.uint8, pin_memory=True)
+        bits_host = torch.empty(used_bits, dtype=torch.int32, pin_memory=True)
+        gaps_host = torch.empty(used_gaps, dtype=torch.int32, pin_memory=True)
+
+        def e2e_step():
+            flat.copy_(in_host, non_blocking=True)                          # H2D inputs
+            g_c.replay()                                                    # compress
+            ent_host.copy_(plan.entries, non_blocking=True)                # D2H entries + streams
+            bits_host.copy_(plan.bits[:used_bits], non_blocking=True)
+            gaps_host.copy_(plan.gaps[:used_gaps], non_blocking=True)
+            plan.entries.copy_(ent_host, non_blocking=True)                # H2D for decompress
+            plan.bits[:used_bits].copy_(bits_host, non_blocking=True)
+            plan.gaps[:used_gaps].copy_(gaps_host, non_blocking=True)
+            g_d.replay()                                                    # decompress
+            out_host.copy_(flat_out, non_blocking=True)                     # D2H outputs
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        e2e_steps = max(2, args.steps // 2)
+        a = torch.cuda.Event(enable_timing=True)
+        b_ = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(e2e_steps):
+            e2e_step()
+        b_.record(stream)
+        torch.cuda.synchronize()
+        e_ms = a.elapsed_time(b_)
+        plan.check()
+        if not torch.equal(out_host, in_host):
+            raise SystemExit("e2e round trip mismatch")
+        if pg:
+            tm = torch.tensor([e_ms], device=dev)
+            pg.all_reduce(tm, op=pg.ReduceOp.MAX)
+            e_ms = float(tm.item())
+        meta = plan.entries.numel()
+        e2e = {"value": round(world * total * e2e_steps / e_ms / 1e6, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": total + 4 * (used_bits + used_gaps) + meta,
+               "d2h_bytes_per_step": 4 * (used_bits + used_gaps) + meta + total,
+               "ms_per_step": round(e_ms / e2e_steps, 3)}
+        del in_host, out_host
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = host_threads()
+        fh = flat.cpu().numpy()
+        budget = args.cpu_sample_mib << 20
+        cpu_batch_sample(sizes, fh, threads, budget // 16)
+        done, dt = cpu_batch_sample(sizes, fh, threads, budget)
+        cpu = {"value": round(done / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": f"the batch's first buffers up to {budget >> 20} MiB ({done} bytes), one "
+                         f"histogram+codebook+encode+decode round trip per buffer (oracle/hgap_oracle.c, pthreads)"}
+
+    if rank == 0:
+        value = world * total * args.steps / ms / 1e6
+        line = {
+            "metric": METRIC,
+            "value": round(value, 3),
+            "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8", "data": "synthetic",
+            "config": {"workload": desc, "buffers": len(sizes), "bytes_per_gpu": total,
+                       "parallelism": f"replicas x{world}",
+                       "step": "batched compress (device histograms, codebooks, encode) then batched "
+                               "decompress, two captured CUDA graphs",
+                       "l2": "inputs (2.46 GB) larger than the 126 MB L2; no flush",
+                       "compressed_bytes": C, "compressed_over_raw": round(C / total, 4),
+                       "tuning": tuning},
+            "encode_gbs": round(total / c_ms / 1e6, 1),
+            "decode_gbs": round(total / d_ms / 1e6, 1),
+            "plain": plain,
+            "speedup_vs_plain": (round(value / world / plain["roundtrip_gbs"], 2)
+                                 if plain else None),
+            "kernels": kernels,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": 16 * args.steps,
+            "clocks": clock_info,
+        }
+        print(json.dumps(line), flush=True)
 
 
 def main():
@@ -213,6 +488,13 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=dev)
         pg = dist
+
+    if args.workload == "batch4096":
+        run_batch(args, rank, world, dev, pg)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
 
     desc, n = WORKLOADS[args.workload]
     x = make_workload(args.workload, dev, rank)

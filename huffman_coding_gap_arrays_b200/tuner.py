@@ -1,0 +1,141 @@
+"""Launch-configuration autotuner for the batched path.
+
+The batched kernels take a launch shape (``LaunchConfig``: encoder region
+size, CTAs per SM of the histogram, encoder and decoder grids) that never
+changes their output.  The autotuner times candidate shapes on the caller's
+own buffers with CUDA events and keeps every measurement as a record
+(buffer features, config, time), which is also the training set of the
+learned tuner (``mlp.py``).
+
+Features of a buffer (cheap, from its histogram and codebook):
+  log2 of its size, its entropy in bits per byte, its longest code length and
+  the fraction of its bytes whose code is longer than the decoder's 11-bit
+  level-1 prefix (level-2 lookups, the decoder's slow path).
+"""
+from __future__ import annotations
+
+import itertools
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .batch import BatchCodec, LaunchConfig
+
+REGIONS = (1, 2, 4, 8, 16, 32)
+HIST_CTAS = (2, 4)
+ENC_CTAS = (1, 2)
+DEC_CTAS = (1, 2, 3)
+
+
+def compress_space():
+    return [LaunchConfig(region_chunks=r, hist_ctas_per_sm=h, enc_ctas_per_sm=e)
+            for r, h, e in itertools.product(REGIONS, HIST_CTAS, ENC_CTAS)]
+
+
+def features_from_hist(n: int, hist: np.ndarray, lengths: np.ndarray) -> np.ndarray:
+    """[log2 n, entropy (bits/byte), max code length, level-2 byte fraction]."""
+    h = np.asarray(hist, np.float64)
+    tot = h.sum()
+    if tot <= 0:
+        return np.array([math.log2(max(n, 1)), 0.0, 0.0, 0.0], np.float32)
+    p = h[h > 0] / tot
+    ent = float(-(p * np.log2(p)).sum())
+    ln = np.asarray(lengths, np.float64)
+    maxlen = float(ln.max()) if ln.size else 0.0
+    l2 = float(h[ln > 11].sum() / tot)
+    return np.array([math.log2(max(n, 1)), ent, maxlen, l2], np.float32)
+
+
+def buffer_features(x: torch.Tensor) -> np.ndarray:
+    """Features of one uint8 CUDA buffer (histogram on the device)."""
+    from . import codec
+    n = x.numel()
+    if n == 0:
+        return np.zeros(4, np.float32)
+    hist = codec.histogram(x).cpu().numpy().view(np.uint32)
+    book, _ = codec.Codebook.from_histogram(hist)
+    return features_from_hist(n, hist, book.length)
+
+
+@dataclass
+class Record:
+    features: np.ndarray   # per buffer (single-buffer runs) or the batch mean
+    config: LaunchConfig
+    compress_ms: float
+    decompress_ms: float
+
+
+@dataclass
+class TuneResult:
+    compress: LaunchConfig
+    decompress_ctas: int
+    compress_ms: float
+    decompress_ms: float
+    records: list = field(default_factory=list)
+
+    @property
+    def config(self) -> LaunchConfig:
+        c = self.compress
+        return LaunchConfig(c.region_chunks, c.hist_ctas_per_sm, c.enc_ctas_per_sm, self.decompress_ctas)
+
+
+def _time(fn, reps: int, warmup: int) -> float:
+    for _ in range(warmup):
+        fn()
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(reps):
+        fn()
+    b.record(s)
+    b.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+class Autotuner:
+    """Exhaustive search of the launch space on the caller's buffers."""
+
+    def __init__(self, reps: int = 3, warmup: int = 1, space=None, dec_space=DEC_CTAS):
+        self.reps = reps
+        self.warmup = warmup
+        self.space = list(space) if space is not None else compress_space()
+        self.dec_space = tuple(dec_space)
+        self.records: list[Record] = []
+
+    def tune(self, inputs, outputs, features: np.ndarray | None = None,
+             plan: BatchCodec | None = None) -> TuneResult:
+        """Times every compress shape, then every decoder grid on the best
+        compress output; every run is checked by the device status."""
+        sizes = [int(t.numel()) for t in inputs]
+        if plan is None:
+            base = min(c.region_chunks for c in self.space)
+            plan = BatchCodec(sizes, LaunchConfig(region_chunks=base))
+            plan.bind(inputs, outputs)
+        feats = features if features is not None else np.zeros(4, np.float32)
+        best_c, best_ms = None, float("inf")
+        for cfg in self.space:
+            plan.config = cfg
+            ms = _time(plan.compress, self.reps, self.warmup)
+            plan.check_compress()
+            self.records.append(Record(feats, cfg, ms, float("nan")))
+            if ms < best_ms:
+                best_c, best_ms = cfg, ms
+        plan.config = best_c
+        plan.compress()
+        plan.check_compress()
+        best_d, best_dms = None, float("inf")
+        for d in self.dec_space:
+            plan.config = LaunchConfig(best_c.region_chunks, best_c.hist_ctas_per_sm, best_c.enc_ctas_per_sm, d)
+            ms = _time(plan.decompress, self.reps, self.warmup)
+            plan.check_decompress()
+            self.records.append(Record(feats, plan.config, float("nan"), ms))
+            if ms < best_dms:
+                best_d, best_dms = d, ms
+        plan.config = LaunchConfig(best_c.region_chunks, best_c.hist_ctas_per_sm, best_c.enc_ctas_per_sm, best_d)
+        return TuneResult(best_c, best_d, best_ms, best_dms, list(self.records))
+
+
+__all__ = ["Autotuner", "TuneResult", "Record", "compress_space", "buffer_features", "features_from_hist",
+           "REGIONS", "HIST_CTAS", "ENC_CTAS", "DEC_CTAS"]
