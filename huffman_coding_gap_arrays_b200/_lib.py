@@ -29,7 +29,8 @@ EXPORTS = [
     "hgap_ref_decoder_l1_l2", "hgap_decode_noalloc", "hgap_codebook_build_device",
     "hgap_decode_table_build", "hgap_decode_table_build_device", "hgap_batch_compress_workspace_bytes",
     "hgap_batch_decompress_workspace_bytes", "hgap_batch_bits_capacity", "hgap_batch_gaps_capacity",
-    "hgap_batch_compress", "hgap_batch_decompress", "hgap_batch_status",
+    "hgap_batch_compress", "hgap_batch_decompress", "hgap_batch_status", "hgap_mlp_forward",
+    "hgap_mlp_loss_grad", "hgap_mlp_adam",
 ]
 
 
@@ -70,6 +71,8 @@ class BatchConfig(C.Structure):
 
 DEC_T1_ENTRIES = 2048
 DEC_T2_ENTRIES = 2560
+MLP_IN, MLP_HIDDEN, MLP_OUT = 8, 32, 2
+MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_OUT * MLP_HIDDEN + MLP_OUT
 
 
 _lib = None
@@ -132,8 +135,12 @@ def lib() -> C.CDLL:
     L.hgap_batch_decompress.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, C.c_size_t,
                                         C.POINTER(BatchConfig), vp]
     L.hgap_batch_status.argtypes = [vp, vp]
+    L.hgap_mlp_forward.argtypes = [vp, vp, C.c_uint32, vp, vp]
+    L.hgap_mlp_loss_grad.argtypes = [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, vp]
+    L.hgap_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, vp]
     for name in ("hgap_codebook_build_device", "hgap_decode_table_build", "hgap_decode_table_build_device",
-                 "hgap_batch_compress", "hgap_batch_decompress", "hgap_batch_status"):
+                 "hgap_batch_compress", "hgap_batch_decompress", "hgap_batch_status", "hgap_mlp_forward",
+                 "hgap_mlp_loss_grad", "hgap_mlp_adam"):
         getattr(L, name).restype = C.c_int
     for name in ("hgap_histogram", "hgap_codebook_build", "hgap_codebook_from_symbols",
                  "hgap_encode", "hgap_encode_histogram", "hgap_encode_prepared", "hgap_decode", "hgap_workspace_status", "hgap_container_write",

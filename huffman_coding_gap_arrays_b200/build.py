@@ -22,7 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-Wall",
          "-Wno-deprecated-gpu-targets", "-I" + os.path.join(ROOT, "include")]
 
-SOURCES = ["hist.cu", "encode.cu", "decode.cu", "api.cu", "batch.cu", "compat.cu", "noalloc.cu", "host.cpp"]
+SOURCES = ["hist.cu", "encode.cu", "decode.cu", "api.cu", "batch.cu", "mlp.cu", "compat.cu", "noalloc.cu",
+           "host.cpp"]
 HEADERS = ["hgap_internal.h", "device_util.cuh", "book.cuh"]
 
 

@@ -10,7 +10,9 @@ learned tuner (``mlp.py``).
 Features of a buffer (cheap, from its histogram and codebook):
   log2 of its size, its entropy in bits per byte, its longest code length and
   the fraction of its bytes whose code is longer than the decoder's 11-bit
-  level-1 prefix (level-2 lookups, the decoder's slow path).
+  level-1 prefix (level-2 lookups, the decoder's slow path).  A batch has the
+  same four, over all its bytes: log2 of its total size and the byte-weighted
+  means of the other three.
 """
 from __future__ import annotations
 
@@ -59,9 +61,28 @@ def buffer_features(x: torch.Tensor) -> np.ndarray:
     return features_from_hist(n, hist, book.length)
 
 
+def batch_features(inputs) -> np.ndarray:
+    """Features of a batch of uint8 CUDA buffers (histograms on the device)."""
+    from . import codec
+    sizes = [int(t.numel()) for t in inputs]
+    total = sum(sizes)
+    if total == 0:
+        return np.zeros(4, np.float32)
+    hs = torch.stack([torch.bincount(t, minlength=256) if t.numel() else
+                      torch.zeros(256, dtype=torch.int64, device=t.device) for t in inputs]).cpu().numpy()
+    acc = np.zeros(3)
+    for n, h in zip(sizes, hs):
+        if n == 0:
+            continue
+        book, _ = codec.Codebook.from_histogram(h.astype(np.uint32))
+        f = features_from_hist(n, h, book.length)
+        acc += n * f[1:]
+    return np.concatenate([[math.log2(total)], acc / total]).astype(np.float32)
+
+
 @dataclass
 class Record:
-    features: np.ndarray   # per buffer (single-buffer runs) or the batch mean
+    features: np.ndarray   # of the tuned input (one buffer, or a batch)
     config: LaunchConfig
     compress_ms: float
     decompress_ms: float
@@ -137,5 +158,6 @@ class Autotuner:
         return TuneResult(best_c, best_d, best_ms, best_dms, list(self.records))
 
 
-__all__ = ["Autotuner", "TuneResult", "Record", "compress_space", "buffer_features", "features_from_hist",
+__all__ = ["Autotuner", "TuneResult", "Record", "compress_space", "buffer_features", "batch_features",
+           "features_from_hist",
            "REGIONS", "HIST_CTAS", "ENC_CTAS", "DEC_CTAS"]

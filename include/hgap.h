@@ -258,6 +258,28 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
  * this workspace, like hgap_workspace_status. */
 hgap_status hgap_batch_status(const void* d_workspace, hgap_stream_t stream);
 
+/* --------------------------------------------------------- learned launch tuner
+ * No counterpart in the reference.  A small MLP (8 inputs -> 32 ReLU -> 32
+ * ReLU -> 2 outputs, fp32) that predicts the log times of the batched
+ * compress and decompress from a batch's features and a launch shape,
+ * trained and run on the GPU by these kernels.  Parameters: one flat array of
+ * HGAP_MLP_PARAMS floats, W1[32][8] b1[32] W2[32][32] b2[32] W3[2][32] b3[2].
+ * d_x: n x 8 inputs, d_y / d_target: n x 2 (NaN targets are unmeasured and
+ * carry no loss).  loss = scale * sum (y - t)^2 / 2; hgap_mlp_loss_grad
+ * overwrites d_grad (HGAP_MLP_PARAMS floats) and *d_loss.  Adam with bias
+ * correction for step >= 1. */
+#define HGAP_MLP_IN 8
+#define HGAP_MLP_HIDDEN 32
+#define HGAP_MLP_OUT 2
+#define HGAP_MLP_PARAMS (HGAP_MLP_HIDDEN * HGAP_MLP_IN + HGAP_MLP_HIDDEN + HGAP_MLP_HIDDEN * HGAP_MLP_HIDDEN + \
+                         HGAP_MLP_HIDDEN + HGAP_MLP_OUT * HGAP_MLP_HIDDEN + HGAP_MLP_OUT)
+hgap_status hgap_mlp_forward(const float* d_params, const float* d_x, uint32_t n, float* d_y,
+                             hgap_stream_t stream);
+hgap_status hgap_mlp_loss_grad(const float* d_params, const float* d_x, const float* d_target, uint32_t n,
+                               float scale, float* d_grad, float* d_loss, hgap_stream_t stream);
+hgap_status hgap_mlp_adam(float* d_params, const float* d_grad, float* d_m, float* d_v, uint32_t step,
+                          float lr, float beta1, float beta2, float eps, hgap_stream_t stream);
+
 /* ------------------------------------------------------------------ container
  * Writer encoder/src/huff.cpp:111-125, reader decoder/src/huff.cpp:27-81:
  * u64 symbol_count; symbol_count x {u8 symbol, u8 length}; u32 n; u32 W;
