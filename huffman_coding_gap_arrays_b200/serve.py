@@ -1,0 +1,305 @@
+"""Serving: a request loop with continuous batching (no counterpart in the
+reference).
+
+Requests -- compress a device buffer, or decompress a stream produced by the
+batched path -- arrive over time.  The loop, running on the host:
+
+  * admits arrived requests, oldest first, into the next batch while the
+    batch stays under ``max_batch`` requests and the device memory the
+    in-flight batches hold stays under the HBM budget;
+  * launches each batch as one batched compress and/or one batched
+    decompress on its own stream (up to ``max_inflight`` batches at once,
+    so requests that arrive while others are on the GPU start as soon as a
+    slot and memory free up, and their work overlaps on the device);
+  * retires batches whose completion event has fired, releasing their
+    memory and stamping their requests' completion times.
+
+Codebooks and decoder tables are built on the device inside each batch and
+never leave it.  Payloads and results stay in HBM (the latency is queueing
+plus GPU service, not network or PCIe time).  The launch shape of each batch
+comes from a ``LearnedTuner`` (its features: the batch's size and the
+traffic's measured byte statistics), from one fixed shape, or -- for
+comparison -- requests run one by one through the plain single-buffer path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import codec
+from ._lib import BatchEntry, check, lib
+from .batch import ENTRY_BYTES, BatchCodec, LaunchConfig
+from .codec import _stream
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float                      # seconds after the start of the run
+    kind: str                           # "compress" | "decompress"
+    data: torch.Tensor | None = None    # compress: uint8 device buffer
+    stream: "EncodedStream | None" = None  # decompress: what to decode
+    # filled by the server
+    start: float = float("nan")         # launch time of its batch
+    done: float = float("nan")          # completion time
+    result: object = None
+
+    @property
+    def nbytes(self) -> int:
+        return int(self.data.numel()) if self.kind == "compress" else int(self.stream.entry.n)
+
+
+@dataclass
+class EncodedStream:
+    """One buffer's encoded stream in device memory, as the batched path
+    produced it (entry with sizes and codebook, bitstream and gap array)."""
+    entry: BatchEntry
+    bits: torch.Tensor   # int32 view of u32 words, 16-byte aligned start
+    gaps: torch.Tensor
+    owner: object = None  # keeps the arenas the views point into alive
+
+    def to_compressed(self):
+        e = self.entry
+        syms = np.array([e.symbols[k].symbol for k in range(e.symbol_count)], np.uint8)
+        lens = np.array([e.symbols[k].length for k in range(e.symbol_count)], np.uint8)
+        book = codec.Codebook.from_symbols(syms, lens)
+        sizes = codec.StreamSizes(int(e.bits), int(e.words), int(e.segments), int(e.gap_words))
+        return codec.Compressed(book, int(e.n), sizes, self.bits, self.gaps)
+
+
+@dataclass
+class _Batch:
+    reqs: list
+    stream: torch.cuda.Stream
+    event: torch.cuda.Event
+    reserved: int
+    keep: list = field(default_factory=list)
+    entries_host: torch.Tensor | None = None
+    plan: BatchCodec | None = None
+    dec_ws: torch.Tensor | None = None
+
+
+class Server:
+    """Continuous-batching request loop on one GPU."""
+
+    def __init__(self, policy: str = "batched", tuner=None, config: LaunchConfig | None = None,
+                 hbm_budget: float = 40e9, max_batch: int = 64, max_inflight: int = 3,
+                 traffic_features=(5.0, 12.0, 0.05), device="cuda", keep_results: bool = False):
+        if policy not in ("batched", "plain"):
+            raise ValueError("policy is 'batched' or 'plain'")
+        self.policy = policy
+        self.tuner = tuner
+        self.config = config or LaunchConfig()
+        self.budget = float(hbm_budget)
+        self.max_batch = int(max_batch)
+        self.max_inflight = int(max_inflight)
+        self.traffic = np.asarray(traffic_features, np.float32)
+        self.device = torch.device(device)
+        self.keep_results = keep_results
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.max_inflight)]
+        self.held = 0
+        self.peak_held = 0
+        self.batches = 0
+
+    # --------------------------------------------------------------- memory
+    @staticmethod
+    def footprint(r: Request) -> int:
+        """Device bytes a request holds while its batch is in flight: the
+        worst-case output arena and workspace for compress, the output and
+        workspace for decompress."""
+        n = r.nbytes
+        if r.kind == "compress":
+            return 2 * n + n // 4 + (1 << 20)
+        return n + n // 64 + (1 << 20)
+
+    def _config_for(self, reqs) -> LaunchConfig:
+        if self.tuner is None:
+            return self.config
+        total = max(1, sum(r.nbytes for r in reqs))
+        f = np.concatenate([[np.log2(total)], self.traffic]).astype(np.float32)
+        return self.tuner.choose(f)
+
+    # -------------------------------------------------------------- batches
+    def _launch(self, reqs, t0) -> _Batch:
+        s = self.streams[self.batches % len(self.streams)]
+        self.batches += 1
+        now = time.perf_counter() - t0
+        for r in reqs:
+            r.start = now
+        reserved = sum(self.footprint(r) for r in reqs)
+        b = _Batch(reqs, s, torch.cuda.Event(), reserved)
+        cfg = self._config_for(reqs)
+        comp = [r for r in reqs if r.kind == "compress"]
+        dec = [r for r in reqs if r.kind == "decompress"]
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            if comp:
+                plan = BatchCodec([r.data.numel() for r in comp], cfg, device=self.device)
+                plan.bind([r.data for r in comp])
+                plan.compress(stream=s)
+                ent = torch.empty(plan.entries.numel(), dtype=torch.uint8, pin_memory=True)
+                ent.copy_(plan.entries, non_blocking=True)
+                b.plan, b.entries_host = plan, ent
+                b.keep.append((comp, plan, ent))
+            if dec:
+                outs = [torch.empty(max(r.nbytes, 1), dtype=torch.uint8, device=self.device) for r in dec]
+                self._decompress(dec, outs, cfg, s, b)
+                for r, o in zip(dec, outs):
+                    r.result = o[:r.nbytes]
+        b.event.record(s)
+        return b
+
+    def _decompress(self, reqs, outs, cfg, s, b) -> None:
+        """One batched decompress over streams that live anywhere in device
+        memory: each entry's offsets are rebased on the lowest address."""
+        count = len(reqs)
+        base_b = min(r.stream.bits.data_ptr() for r in reqs) & ~15
+        base_g = min(r.stream.gaps.data_ptr() for r in reqs) & ~3
+        arr = (BatchEntry * count)()
+        for i, r in enumerate(reqs):
+            C.memmove(C.byref(arr[i]), C.byref(r.stream.entry), ENTRY_BYTES)
+            arr[i].bits_offset = (r.stream.bits.data_ptr() - base_b) // 4
+            arr[i].gaps_offset = (r.stream.gaps.data_ptr() - base_g) // 4
+        host = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8)
+        d_ent = host.to(self.device, non_blocking=False)
+        d_out = torch.tensor([o.data_ptr() for o in outs], dtype=torch.int64).to(self.device)
+        sizes = np.array([r.nbytes for r in reqs], np.uint64)
+        nbytes = lib().hgap_batch_decompress_workspace_bytes(count, sizes.ctypes.data_as(C.POINTER(C.c_uint64)))
+        ws = torch.empty((nbytes + 7) // 8, dtype=torch.int64, device=self.device)
+        c = cfg.cstruct()
+        check(lib().hgap_batch_decompress(count, d_ent.data_ptr(), base_b, base_g, d_out.data_ptr(),
+                                          ws.data_ptr(), ws.numel() * 8, C.byref(c), _stream(s)),
+              "hgap_batch_decompress")
+        b.keep.append((reqs, d_ent, d_out, ws, outs))
+        b.dec_ws = ws
+
+    def _retire(self, b: _Batch, now: float) -> None:
+        # device status of the batch's launches (the event has fired: no wait)
+        if b.plan is not None:
+            check(lib().hgap_batch_status(b.plan.enc_ws.data_ptr(), _stream(b.stream)), "served compress")
+        if b.dec_ws is not None:
+            check(lib().hgap_batch_status(b.dec_ws.data_ptr(), _stream(b.stream)), "served decompress")
+        for r in b.reqs:
+            r.done = now
+        if b.plan is not None:
+            comp = [r for r in b.reqs if r.kind == "compress"]
+            raw = b.entries_host.numpy().tobytes()
+            arr = (BatchEntry * len(comp)).from_buffer_copy(raw[:ENTRY_BYTES * len(comp)])
+            for i, r in enumerate(comp):
+                e = arr[i]
+                bits = b.plan.bits[e.bits_offset:e.bits_offset + e.words]
+                gaps = b.plan.gaps[e.gaps_offset:e.gaps_offset + e.gap_words]
+                r.result = EncodedStream(e, bits, gaps, b.plan) if self.keep_results else int(e.words)
+        if not self.keep_results:
+            for r in b.reqs:
+                if r.kind == "decompress":
+                    r.result = None  # the output is released with the batch
+        self.held -= b.reserved
+
+    # ---------------------------------------------------------------- loop
+    def run(self, requests) -> dict:
+        """Serves `requests` (sorted by arrival) in real time; returns the
+        latency and throughput statistics."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        if self.policy == "plain":
+            return self._run_plain(reqs)
+        pending = deque(reqs)
+        queue = deque()
+        inflight = []
+        torch.cuda.synchronize(self.device)
+        t0 = time.perf_counter()
+        while pending or queue or inflight:
+            now = time.perf_counter() - t0
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.popleft())
+            for b in list(inflight):
+                if b.event.query():
+                    inflight.remove(b)
+                    self._retire(b, time.perf_counter() - t0)
+            if queue and len(inflight) < self.max_inflight:
+                take, mem = [], 0
+                while queue and len(take) < self.max_batch:
+                    f = self.footprint(queue[0])
+                    if self.held + mem + f > self.budget and (take or inflight):
+                        break  # wait for memory to free up
+                    take.append(queue.popleft())
+                    mem += f
+                if take:
+                    b = self._launch(take, t0)
+                    self.held += b.reserved
+                    self.peak_held = max(self.peak_held, self.held)
+                    inflight.append(b)
+                    continue
+            if not queue and not inflight and pending:
+                time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 1e-3)))
+        t_end = time.perf_counter() - t0
+        return self._stats(reqs, t_end)
+
+    def _run_plain(self, reqs) -> dict:
+        """Each request alone through the single-buffer path, in arrival order."""
+        torch.cuda.synchronize(self.device)
+        t0 = time.perf_counter()
+        for r in reqs:
+            now = time.perf_counter() - t0
+            if r.arrival > now:
+                time.sleep(r.arrival - now)
+            r.start = time.perf_counter() - t0
+            if r.kind == "compress":
+                c = codec.compress(r.data)
+                r.result = c if self.keep_results else int(c.sizes.words)
+            else:
+                r.result = codec.decompress(r.stream.to_compressed())
+            torch.cuda.synchronize(self.device)
+            r.done = time.perf_counter() - t0
+        return self._stats(reqs, time.perf_counter() - t0)
+
+    def _stats(self, reqs, t_end) -> dict:
+        lat = np.array([r.done - r.arrival for r in reqs]) * 1e3
+        total = sum(r.nbytes for r in reqs)
+        return {"requests": len(reqs), "bytes": total, "seconds": round(t_end, 4),
+                "sustained_gbs": round(total / t_end / 1e9, 3),
+                "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                "mean_ms": round(float(lat.mean()), 3), "batches": self.batches,
+                "peak_hbm_gb": round(self.peak_held / 1e9, 3)}
+
+
+def poisson_requests(count: int, rate_gbs: float, pool: torch.Tensor, streams: list, seed: int = 5,
+                     lo: int = 64 << 10, hi: int = 64 << 20, decompress_frac: float = 0.5) -> list:
+    """`count` requests with log-uniform sizes in [lo, hi], Poisson arrivals at
+    `rate_gbs` of offered load; compress requests are slices of `pool`,
+    decompress requests pick one of the pre-encoded `streams`."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(np.int64)
+    mean = float(sizes.mean())
+    lam = rate_gbs * 1e9 / mean
+    t = np.cumsum(rng.exponential(1.0 / lam, count))
+    out = []
+    for i in range(count):
+        if streams and rng.random() < decompress_frac:
+            s = streams[int(rng.integers(len(streams)))]
+            out.append(Request(i, float(t[i]), "decompress", stream=s))
+        else:
+            n = int(min(sizes[i], pool.numel()))
+            off = int(rng.integers(0, pool.numel() - n + 1))
+            out.append(Request(i, float(t[i]), "compress", data=pool[off:off + n]))
+    return out
+
+
+def encode_streams(buffers, config: LaunchConfig | None = None) -> list:
+    """Pre-encodes buffers with the batched path (the decompress payloads)."""
+    plan = BatchCodec([b.numel() for b in buffers], config)
+    plan.bind(buffers)
+    plan.compress()
+    plan.check_compress()
+    ents = plan.entries_host()
+    return [EncodedStream(e, plan.bits[e.bits_offset:e.bits_offset + e.words],
+                          plan.gaps[e.gaps_offset:e.gaps_offset + e.gap_words], plan) for e in ents]
+
+
+__all__ = ["Server", "Request", "EncodedStream", "poisson_requests", "encode_streams"]
