@@ -60,7 +60,10 @@ def parse():
     p.add_argument("--workload", default="batch4096", choices=sorted(WORKLOADS))
     p.add_argument("--plain-buffers", type=int, default=4096,
                    help="buffers of the batch timed through the plain per-buffer path")
-    p.add_argument("--no-tune", action="store_true", help="skip the autotuner: fixed default config")
+    p.add_argument("--no-tune", action="store_true", help="skip tuning: fixed default launch shape")
+    p.add_argument("--serve-requests", type=int, default=1500,
+                   help="requests of the serving run (0: none); the full stream is 100000")
+    p.add_argument("--serve-gbs", type=float, default=20.0, help="offered load of the serving run")
     p.add_argument("--cpu-sample-mib", type=int, default=256)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -261,6 +264,74 @@ def run_reference(args, rank: int, world: int):
     del torch
 
 
+def train_learned_tuner(dev):
+    """The learned tuner, trained on the autotuner's records of batches drawn
+    from the same distributions as the workload but with other seeds, counts
+    and size ranges (it never sees the timed batch)."""
+    import torch
+    from huffman_coding_gap_arrays_b200 import mlp as ML
+    from huffman_coding_gap_arrays_b200 import tuner as T
+    from huffman_coding_gap_arrays_b200 import workloads as WL
+    shapes = [(64, 64 << 10), (256, 256 << 10), (512, 1 << 20), (128, 4 << 20), (1024, 4 << 20),
+              (2048, 1 << 20), (32, 16 << 20), (384, 2 << 20), (1536, 512 << 10), (768, 4 << 20),
+              (96, 8 << 20), (2048, 4 << 20)]
+    hold = [(200, 2 << 20), (1200, 4 << 20)]
+
+    def records(sh, seed):
+        recs = []
+        for k, (count, hi) in enumerate(sh):
+            sz = WL.batch_sizes(count, lo=4096, hi=hi, seed=seed + k)
+            bufs = [WL.batch_buffer(n, (seed + k) * 7919 + i, device=dev) for i, n in enumerate(sz)]
+            outs = [torch.empty_like(b) for b in bufs]
+            recs.extend(T.Autotuner(reps=2, warmup=1).tune(bufs, outs, T.batch_features(bufs)).records)
+            del bufs, outs
+        return recs
+
+    lt = ML.LearnedTuner.train(records(shapes, 9500), holdout=records(hold, 9600), steps=3000)
+    torch.cuda.empty_cache()
+    return lt
+
+
+def picks_cfg(tuning):
+    from huffman_coding_gap_arrays_b200 import batch as B
+    m = tuning.get("measured", {})
+    if "autotuner" in m:
+        return B.LaunchConfig(**m["autotuner"]["config"])
+    return B.LaunchConfig(**tuning["config"])
+
+
+def run_serving(args, pool, learned, fixed_cfg, dev):
+    """Serving at `--serve-gbs` offered load: the learned tuner, the one shape
+    the exhaustive search chose for the batched workload, and the plain
+    per-request path, each on the same request stream."""
+    import numpy as np
+    import torch
+    from huffman_coding_gap_arrays_b200 import serve as SV
+    from huffman_coding_gap_arrays_b200 import tuner as T
+    rng = np.random.default_rng(17)
+    bufs = []
+    for _ in range(32):  # decompress payloads: slices of the pool, pre-encoded
+        n = int(np.exp(rng.uniform(np.log(64 << 10), np.log(64 << 20))))
+        off = int(rng.integers(0, pool.numel() - n))
+        bufs.append(pool[off:off + n])
+    streams = SV.encode_streams(bufs)
+    traffic = T.batch_features(bufs)[1:]
+    out = {"requests": args.serve_requests, "offered_gbs": args.serve_gbs, "hbm_budget_gb": 40,
+           "sizes": "log-uniform 64 KiB .. 64 MiB, 50/50 compress/decompress, Poisson arrivals",
+           "where": "payloads and results resident in HBM; latency = queueing + GPU service"}
+    policies = [("autotuner_fixed", dict(config=fixed_cfg))]
+    if learned is not None and learned.usable:
+        policies.insert(0, ("mlp", dict(tuner=learned)))
+    policies.append(("plain", dict(policy="plain")))
+    for name, kw in policies:
+        reqs = SV.poisson_requests(args.serve_requests, args.serve_gbs, pool, streams, seed=23)
+        srv = SV.Server(hbm_budget=40e9, traffic_features=traffic, device=dev, **kw)
+        out[name] = srv.run(reqs)
+        del reqs
+        torch.cuda.synchronize()
+    return out
+
+
 def run_batch(args, rank, world, dev, pg):
     """The batched path on the 4096-buffer workload (see the module docstring)."""
     import numpy as np
@@ -278,20 +349,39 @@ def run_batch(args, rank, world, dev, pg):
         outs.append(flat_out[p:p + n])
         p += n
 
-    # ---- tuning (untimed): exhaustive search of the launch space ------------
+    # ---- tuning (untimed): learned tuner, checked against the exhaustive search
+    plan = B.BatchCodec(sizes, B.LaunchConfig(region_chunks=1), device=dev)  # workspace fits every shape
+    plan.bind(ins, outs)
+    tuning = {}
+    learned = None
     if args.no_tune:
         cfg = B.LaunchConfig()
-        tuning = {"method": "fixed default", "config": vars(cfg)}
+        tuning["method"] = "fixed default"
     else:
         t0 = time.time()
-        res = T.Autotuner(reps=2, warmup=1).tune(ins, outs)
-        cfg = res.config
-        tuning = {"method": "autotuner (exhaustive)", "config": vars(cfg),
-                  "candidates": len(T.compress_space()) + len(T.DEC_CTAS),
-                  "seconds": round(time.time() - t0, 2)}
-        torch.cuda.empty_cache()
-    plan = B.BatchCodec(sizes, cfg, device=dev)
-    plan.bind(ins, outs)
+        learned = train_learned_tuner(dev)
+        tuning["learned_train_seconds"] = round(time.time() - t0, 2)
+        tuning["learned_holdout_rmse"] = round(learned.holdout_rmse, 4)
+        feats = T.batch_features(ins)
+        t0 = time.time()
+        res = T.Autotuner(reps=2, warmup=1).tune(ins, outs, feats, plan=plan)
+        tuning["autotuner_seconds"] = round(time.time() - t0, 2)
+        picks = {"default": B.LaunchConfig(), "autotuner": res.config}
+        if learned.usable:
+            picks["mlp"] = learned.choose(feats)
+        measured = {}
+        for name, c in picks.items():
+            plan.config = c
+            cm = T._time(plan.compress, 3, 1)
+            dm = T._time(plan.decompress, 3, 1)
+            plan.check()
+            measured[name] = {"config": vars(c), "compress_ms": round(cm, 4), "decompress_ms": round(dm, 4)}
+        tuning["measured"] = measured
+        cfg = picks["mlp"] if "mlp" in picks else picks["autotuner"]
+        tuning["method"] = ("learned tuner (MLP ensemble trained on autotuner records of other batches)"
+                            if "mlp" in picks else "autotuner (exhaustive; learned tuner not usable)")
+    tuning["config"] = vars(cfg)
+    plan.config = cfg
     plan.compress()
     plan.decompress()
     plan.check()
@@ -424,6 +514,11 @@ def run_batch(args, rank, world, dev, pg):
                "ms_per_step": round(e_ms / e2e_steps, 3)}
         del in_host, out_host
 
+    # ---- serving: a Poisson stream of mixed requests (64 KiB .. 64 MiB) -------
+    serving = None
+    if args.serve_requests and rank == 0:
+        serving = run_serving(args, flat, learned, picks_cfg(tuning), dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = host_threads()
@@ -455,6 +550,7 @@ def run_batch(args, rank, world, dev, pg):
             "encode_gbs": round(total / c_ms / 1e6, 1),
             "decode_gbs": round(total / d_ms / 1e6, 1),
             "plain": plain,
+            "serving": serving,
             "speedup_vs_plain": (round(value / world / plain["roundtrip_gbs"], 2)
                                  if plain else None),
             "kernels": kernels,

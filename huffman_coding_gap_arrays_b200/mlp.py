@@ -145,6 +145,7 @@ class LearnedTuner:
         self.dec_margin = dec_margin  # the decoder grid moves decompress time little: be stricter
         self.default = default or LaunchConfig()
         self.holdout_rmse = float("inf")
+        self._memo = {}  # choices by features rounded to 1/8: a serving loop asks about the same sizes
 
     @classmethod
     def train(cls, records, holdout=None, seeds=(0, 1, 2), steps: int = 3000, **kw) -> "LearnedTuner":
@@ -178,13 +179,18 @@ class LearnedTuner:
     def choose(self, features) -> LaunchConfig:
         """The compress shape with the least predicted compress time, then the
         decoder grid with the least predicted decompress time."""
-        f = np.asarray(features, np.float32)
+        f = np.round(np.asarray(features, np.float32) * 8) / 8
+        key = tuple(f.tolist())
+        if key in self._memo:
+            return self._memo[key]
         d0 = self.default
         c = self._pick(f, self.space, LaunchConfig(d0.region_chunks, d0.hist_ctas_per_sm, d0.enc_ctas_per_sm,
                                                    d0.dec_ctas_per_sm), 0, self.margin)
         dec = [LaunchConfig(c.region_chunks, c.hist_ctas_per_sm, c.enc_ctas_per_sm, d) for d in self.dec_space]
         dd = LaunchConfig(c.region_chunks, c.hist_ctas_per_sm, c.enc_ctas_per_sm, d0.dec_ctas_per_sm)
-        return self._pick(f, dec, dd, 1, self.dec_margin)
+        pick = self._pick(f, dec, dd, 1, self.dec_margin)
+        self._memo[key] = pick
+        return pick
 
     def choose_or_search(self, features, inputs, outputs) -> LaunchConfig:
         """The ensemble's pick when it is trained and accurate enough on
