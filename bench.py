@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="hgap", choices=["hgap", "reference"])
     p.add_argument("--workload", default="batch4096", choices=sorted(WORKLOADS))
+    p.add_argument("--batch-count", type=int, default=4096,
+                   help="buffers of the batched workload (fewer only for profiling captures)")
     p.add_argument("--plain-buffers", type=int, default=4096,
                    help="buffers of the batch timed through the plain per-buffer path")
     p.add_argument("--no-tune", action="store_true", help="skip tuning: fixed default launch shape")
@@ -170,12 +172,13 @@ def make_workload(name: str, device, rank: int = 0):
     return WL.zipf_buffer(16 << 20, 1.2, seed=1 + 1000 * rank, device=device)
 
 
-def batch_workload(device, rank: int = 0):
-    """The 4096 buffers of the batched workload, packed back to back in one
-    device allocation (so the end-to-end copies are one H2D and one D2H)."""
+def batch_workload(device, rank: int = 0, count: int = 4096):
+    """The buffers of the batched workload (4096; fewer for profiling), packed
+    back to back in one device allocation (so the end-to-end copies are one
+    H2D and one D2H)."""
     import torch
     from huffman_coding_gap_arrays_b200 import workloads as WL
-    sizes = WL.batch_sizes(4096, seed=4 + 1000 * rank)
+    sizes = WL.batch_sizes(count, seed=4 + 1000 * rank)
     total = sum(sizes)
     flat = torch.empty(total, dtype=torch.uint8, device=device)
     views, p = [], 0
@@ -219,7 +222,7 @@ def run_reference(args, rank: int, world: int):
     threads = host_threads()
     if args.workload == "batch4096":
         desc = WORKLOADS["batch4096"][0]
-        sizes, flat, _ = batch_workload("cpu")
+        sizes, flat, _ = batch_workload("cpu", 0, args.batch_count)
         fh = flat.numpy()
         budget = args.cpu_sample_mib << 20
         for _ in range(args.warmup):
@@ -341,7 +344,9 @@ def run_batch(args, rank, world, dev, pg):
     from huffman_coding_gap_arrays_b200 import tuner as T
 
     desc = WORKLOADS["batch4096"][0]
-    sizes, flat, ins = batch_workload(dev, rank)
+    if args.batch_count != 4096:
+        desc = desc.replace("4096 uint8 buffers", f"{args.batch_count} uint8 buffers (profiling size)")
+    sizes, flat, ins = batch_workload(dev, rank, args.batch_count)
     total = sum(sizes)
     flat_out = torch.empty(total, dtype=torch.uint8, device=dev)
     outs, p = [], 0
