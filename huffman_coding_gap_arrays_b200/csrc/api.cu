@@ -215,7 +215,9 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
         kraft += 1ull << (hgap::kMaxLen - book.symbols[i].length);
     }
     const bool complete = kraft == (1ull << hgap::kMaxLen);
-    return cuda_status(hgap::launch_decode(a, t, min_len, complete, 0, stream));
+    // two symbols per lookup pay off once about a third of the lookups yield two
+    const bool pairs = hgap::dec_pair_fraction(t) >= 0.3;
+    return cuda_status(hgap::launch_decode(a, t, min_len, complete, pairs, 0, stream));
 }
 
 hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream) {

@@ -602,7 +602,8 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
         a.lookback = records;
         a.counter = counters + c;
         a.status = status;
-        if (launch_decode(a, unused, kMinLen[c / 2], (c & 1) != 0, (int)cfg->dec_ctas_per_sm, stream) != 0)
+        // batched streams are compressible ones on the whole: always two symbols per lookup where they fit
+        if (launch_decode(a, unused, kMinLen[c / 2], (c & 1) != 0, true, (int)cfg->dec_ctas_per_sm, stream) != 0)
             return HGAP_ERR_CUDA;
     }
     return HGAP_OK;

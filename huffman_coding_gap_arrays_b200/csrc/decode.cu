@@ -50,11 +50,29 @@ struct DecCfg {
 };
 
 // Table entry in shared memory (u32): direct = len << 24 | symbol;
-// pointer = bit 31 | extra width << 16 | level-2 offset; invalid = bit 30.
+// pointer = bit 31 | extra width << 16 | level-2 offset; invalid = bit 30;
+// pair (level 1 only, see widen_pair) = two symbols with bit 16 set.
 __device__ __forceinline__ uint32_t widen_entry(uint32_t e) {
     if (e & 0x8000u) return 0x80000000u | (((e >> 12) & 7u) << 16) | (e & 0xfffu);
     if (e & kDecInvalid) return 0x40000000u;
     return ((((e >> 8) & 15u) + 1u) << 24) | (e & 0xffu);
+}
+
+// Level-1 entry in shared memory for prefix x, from the u16 table: when the
+// first code leaves room for a whole second code inside the same 11-bit
+// window, both are returned at once (a pair entry: symbol 1 | symbol 2 << 8 |
+// bit 16 | length 1 << 17 | total length << 24).  The second code is known
+// from the bits after the first alone, because it ends inside the window.
+__device__ __forceinline__ uint32_t widen_pair(const uint16_t* t1src, uint32_t x) {
+    const uint32_t e = widen_entry(t1src[x]);
+    if (e & 0xC0000000u) return e;  // pointer or invalid
+    const uint32_t l1 = e >> 24;
+    if (l1 >= (uint32_t)kDecPrefix) return e;
+    const uint32_t e2 = widen_entry(t1src[(x << l1) & ((1u << kDecPrefix) - 1u)]);
+    if (e2 & 0xC0000000u) return e;
+    const uint32_t l2 = e2 >> 24;
+    if (l1 + l2 > (uint32_t)kDecPrefix) return e;
+    return (e & 0xffu) | ((e2 & 0xffu) << 8) | 0x10000u | (l1 << 17) | ((l1 + l2) << 24);
 }
 
 __device__ __forceinline__ uint32_t pidx(uint32_t w) { return w + (w >> 3); }
@@ -84,7 +102,9 @@ struct DecSlot {
 
 // COMPLETE: the book's Kraft sum is 1 (every package-merge book with two or
 // more symbols), so no table entry is invalid and the decode loop skips that test.
-template <int R, bool COMPLETE>
+// PAIRS: level-1 entries carry two symbols where both codes fit in the window
+// (worth it for short-code books; for long codes the extra selects only cost).
+template <int R, bool COMPLETE, bool PAIRS>
 __global__ void __launch_bounds__(kDecThreads, 3)
     decode_kernel(const __grid_constant__ DecArgs a, const __grid_constant__ DecTable tab) {
     using C = DecCfg<R>;
@@ -103,7 +123,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
 
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     auto load_tables = [&](const DecTable& t) {
-        for (int i = tid; i < C::kT1; i += kDecThreads) t1[i] = widen_entry(t.t1[i]);
+        for (int i = tid; i < C::kT1; i += kDecThreads) t1[i] = PAIRS ? widen_pair(t.t1, i) : widen_entry(t.t1[i]);
         for (int i = tid; i < C::kT2; i += kDecThreads) t2[i] = t.t2[i];
     };
     // thread 0: the tile `item` and its job into slot s
@@ -201,9 +221,21 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                             bad = !last;  // zero padding after the final codeword may not decode
                             break;
                         }
-                        *out = (uint8_t)e;
-                        out += C::kPitch;
-                        pos += e >> 24;
+                        if (PAIRS) {
+                            // one or two symbols; the second only if it starts inside the segment
+                            const uint32_t tot = e >> 24;
+                            const bool pair = (e & 0x10000u) != 0;
+                            const uint32_t l1 = pair ? ((e >> 17) & 15u) : tot;
+                            const bool two = pair && pos + l1 < end;
+                            out[0] = (uint8_t)e;
+                            if (two) out[C::kPitch] = (uint8_t)(e >> 8);
+                            out += two ? 2 * C::kPitch : C::kPitch;
+                            pos += two ? tot : l1;
+                        } else {
+                            *out = (uint8_t)e;
+                            out += C::kPitch;
+                            pos += e >> 24;
+                        }
                     }
                     cnt = (uint32_t)(out - (stage + col)) / C::kPitch;
                     if (!last && !bad && pos != 128 * col + 128 + gap_of(s)) bad = true;
@@ -318,10 +350,10 @@ __global__ void __launch_bounds__(kDecThreads, 3)
 
 uint64_t decode_tiles(uint64_t segments) { return (segments + kDecSegs - 1) / kDecSegs; }
 
-template <int R, bool COMPLETE>
+template <int R, bool COMPLETE, bool PAIRS>
 static int launch_decode_r(const DecArgs& a, const DecTable& t, int ctas_per_sm, cudaStream_t st) {
     using C = DecCfg<R>;
-    auto kern = decode_kernel<R, COMPLETE>;
+    auto kern = decode_kernel<R, COMPLETE, PAIRS>;
     static int sms = 0, per_sm = 0;
     if (sms == 0) {
         int dev = 0;
@@ -339,22 +371,25 @@ static int launch_decode_r(const DecArgs& a, const DecTable& t, int ctas_per_sm,
     return cudaGetLastError();
 }
 
-template <bool COMPLETE>
+template <bool COMPLETE, bool PAIRS>
 static int launch_decode_c(const DecArgs& a, const DecTable& t, uint32_t max_sym, int k, cudaStream_t st) {
-    if (max_sym <= 32) return launch_decode_r<8, COMPLETE>(a, t, k, st);
-    if (max_sym <= 44) return launch_decode_r<11, COMPLETE>(a, t, k, st);
-    if (max_sym <= 64) return launch_decode_r<16, COMPLETE>(a, t, k, st);
-    return launch_decode_r<32, COMPLETE>(a, t, k, st);
+    if (max_sym <= 32) return launch_decode_r<8, COMPLETE, PAIRS>(a, t, k, st);
+    if (max_sym <= 44) return launch_decode_r<11, COMPLETE, PAIRS>(a, t, k, st);
+    if (max_sym <= 64) return launch_decode_r<16, COMPLETE, PAIRS>(a, t, k, st);
+    return launch_decode_r<32, COMPLETE, PAIRS>(a, t, k, st);
 }
 
 // min_len: shortest code length of the book.  A segment holds at most
 // ceil(128 / min_len) codeword starts; the stage is sized for that.
-int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, int ctas_per_sm,
-                  void* stream) {
+int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, bool pairs,
+                  int ctas_per_sm, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const uint32_t max_sym = (128 + min_len - 1) / (min_len ? min_len : 1);
-    return complete ? launch_decode_c<true>(a, t, max_sym, ctas_per_sm, st)
-                    : launch_decode_c<false>(a, t, max_sym, ctas_per_sm, st);
+    if (pairs)
+        return complete ? launch_decode_c<true, true>(a, t, max_sym, ctas_per_sm, st)
+                        : launch_decode_c<false, true>(a, t, max_sym, ctas_per_sm, st);
+    return complete ? launch_decode_c<true, false>(a, t, max_sym, ctas_per_sm, st)
+                    : launch_decode_c<false, false>(a, t, max_sym, ctas_per_sm, st);
 }
 
 }  // namespace hgap

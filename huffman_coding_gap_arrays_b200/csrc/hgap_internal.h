@@ -165,8 +165,12 @@ struct DecArgs {
 int launch_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, void* stream);
 int launch_encode(const EncArgs& a, const EncTable& t, int ctas_per_sm, void* stream);
 int launch_hist_st(const HistStArgs& a, int ctas_per_sm, void* stream);
-int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, int ctas_per_sm,
-                  void* stream);
+int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, bool pairs,
+                  int ctas_per_sm, void* stream);
+// Fraction of level-1 entries that decode two symbols (the decoder's pair
+// rate under the code's own distribution, where every 11-bit prefix is
+// equally likely).
+double dec_pair_fraction(const DecTable& t);
 uint64_t decode_tiles(uint64_t segments);
 
 // ------------------------------------------------------------- host helpers -

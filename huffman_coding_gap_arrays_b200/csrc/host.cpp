@@ -143,6 +143,22 @@ hgap_status make_dec_table(const hgap_codebook& cb, DecTable* t) {
     return HGAP_OK;
 }
 
+double dec_pair_fraction(const DecTable& t) {
+    constexpr uint32_t P = kDecPrefix, mask = (1u << P) - 1u;
+    auto direct_len = [&](uint32_t x) -> uint32_t {  // 0 unless a valid direct entry
+        const uint16_t e = t.t1[x];
+        return (e & 0x8000u) || (e & kDecInvalid) ? 0u : ((e >> 8) & 15u) + 1u;
+    };
+    uint32_t pairs = 0;
+    for (uint32_t x = 0; x <= mask; ++x) {
+        const uint32_t l1 = direct_len(x);
+        if (l1 == 0 || l1 >= P) continue;
+        const uint32_t l2 = direct_len((x << l1) & mask);
+        if (l2 && l1 + l2 <= P) ++pairs;
+    }
+    return pairs / double(mask + 1);
+}
+
 }  // namespace hgap
 
 extern "C" {
