@@ -77,12 +77,9 @@ __device__ __forceinline__ uint32_t widen_pair(const uint16_t* t1src, uint32_t x
 
 __device__ __forceinline__ uint32_t pidx(uint32_t w) { return w + (w >> 3); }
 
-// One codeword of a segment: window from two staged words, level-1 lookup,
-// level 2 for the rare longer codes.  Returns the widened entry.
-__device__ __forceinline__ uint32_t lookup(const uint32_t* sw, const uint32_t* t1,
-                                           const uint16_t* t2, uint32_t pos) {
-    const uint32_t w = pos >> 5;
-    const uint32_t x = __funnelshift_l(sw[pidx(w + 1)], sw[pidx(w)], pos);
+// One codeword from the 32-bit window x at the current position: level-1
+// lookup, level 2 for the rare longer codes.  Returns the widened entry.
+__device__ __forceinline__ uint32_t lookup(const uint32_t* t1, const uint16_t* t2, uint32_t x) {
     uint32_t e = t1[x >> (32 - kDecPrefix)];
     if (e & 0x80000000u) {
         const uint32_t wd = (e >> 16) & 7u;
@@ -213,10 +210,14 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                     if (last && stream_bits - 128 * s0 < end) end = (uint32_t)(stream_bits - 128 * s0);
                     bool bad = false;
                     uint8_t* out = stage + col;
+                    // the window's two stream words live in registers; a code moves
+                    // the position by at most 16 bits, so at most one new word per code
+                    uint32_t w = pos >> 5;
+                    uint32_t cw = sw[pidx(w)], nw = sw[pidx(w + 1)];
                     // every codeword is at least the book's shortest length, so a
                     // segment yields at most kMaxSym symbols: no count test needed
                     while (pos < end) {
-                        const uint32_t e = lookup(sw, t1, t2, pos);
+                        const uint32_t e = lookup(t1, t2, __funnelshift_l(nw, cw, pos));
                         if (!COMPLETE && (e & 0x40000000u)) {
                             bad = !last;  // zero padding after the final codeword may not decode
                             break;
@@ -235,6 +236,11 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                             *out = (uint8_t)e;
                             out += C::kPitch;
                             pos += e >> 24;
+                        }
+                        if ((pos >> 5) != w) {
+                            ++w;
+                            cw = nw;
+                            nw = sw[pidx(w + 1)];
                         }
                     }
                     cnt = (uint32_t)(out - (stage + col)) / C::kPitch;
