@@ -382,20 +382,30 @@ __global__ void __launch_bounds__(kEncThreads, 2)
                 }
                 *reinterpret_cast<uint4*>(img + j) = make_uint4(0, 0, 0, 0);
             }
-            // gap words [P>>10, kn>>3); word kn>>3 is partial (or empty) and carried
+            // gap words [P>>10, kn>>3): one thread per segment k (slot t = k - kb8)
+            // puts its nibble in place, the 8 lanes of a gap word OR them with
+            // shuffles; the word of kn>>3 is partial (or empty) and carried
             const uint64_t kb = P >> 7, kn = E >> 7;  // segments ending in this chunk: [kb, kn)
-            const uint64_t gwb = P >> 10, gwe = kn >> 3;
-            for (uint64_t g = gwb + tid; g <= gwe; g += kEncThreads) {
-                uint32_t v = (g == gwb) ? sh.gcarry[cons & 1] : 0u;
-                const uint64_t k0 = (8 * g > kb) ? 8 * g : kb;
-                const uint64_t k1 = (8 * g + 8 < kn) ? 8 * g + 8 : kn;
-                for (uint64_t k = k0; k < k1; ++k)  // entry k = spill of global word 4k+3
-                    v |= (uint32_t)spills[(uint32_t)(4 * k + 3 - sb)] << (4 * (uint32_t)(k & 7));
-                if (g < gwe) {
-                    if (g < J.gap_words) J.gaps[g] = v;
-                    else overflow = true;
-                } else {
-                    sh.gcarry[(cons + 1) & 1] = v;
+            const uint64_t kb8 = kb & ~7ull;
+            const uint32_t nk = (uint32_t)(8 * ((kn >> 3) - (kb8 >> 3) + 1));
+            for (uint32_t t0 = warp * 32; t0 < nk; t0 += kEncThreads) {  // warp-uniform
+                const uint32_t t = t0 + lane;
+                const uint64_t k = kb8 + t;
+                uint32_t v = 0;
+                if (t < nk && k >= kb && k < kn)  // entry k = spill of global word 4k+3
+                    v = (uint32_t)spills[(uint32_t)(4 * k + 3 - sb)] << (4 * (uint32_t)(k & 7));
+                if (t == 0) v |= sh.gcarry[cons & 1];  // nibbles carried into word kb8 >> 3
+                v |= __shfl_xor_sync(kFull, v, 1);
+                v |= __shfl_xor_sync(kFull, v, 2);
+                v |= __shfl_xor_sync(kFull, v, 4);
+                if (t < nk && (t & 7) == 0) {
+                    const uint64_t g = k >> 3;
+                    if (g < (kn >> 3)) {
+                        if (g < J.gap_words) J.gaps[g] = v;
+                        else overflow = true;
+                    } else {
+                        sh.gcarry[(cons + 1) & 1] = v;
+                    }
                 }
             }
             P = E;
