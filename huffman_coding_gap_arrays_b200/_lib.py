@@ -137,7 +137,8 @@ def lib() -> C.CDLL:
     L.hgap_batch_status.argtypes = [vp, vp]
     L.hgap_mlp_forward.argtypes = [vp, vp, C.c_uint32, vp, vp]
     L.hgap_mlp_loss_grad.argtypes = [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, vp]
-    L.hgap_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float, vp]
+    L.hgap_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float,
+                                C.c_float, vp]
     for name in ("hgap_codebook_build_device", "hgap_decode_table_build", "hgap_decode_table_build_device",
                  "hgap_batch_compress", "hgap_batch_decompress", "hgap_batch_status", "hgap_mlp_forward",
                  "hgap_mlp_loss_grad", "hgap_mlp_adam"):

@@ -164,7 +164,7 @@ hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, u
 }
 
 size_t hgap_decode_workspace_bytes(uint64_t segments) {
-    return kWsHeader + sizeof(uint64_t) * (size_t)hgap::decode_tiles(segments);
+    return kWsHeader + sizeof(uint64_t) * (size_t)hgap::decode_tiles(segments, 1);  // worst case
 }
 
 hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps,
@@ -183,6 +183,12 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     hgap::DecTable t;
     s = hgap::make_dec_table(book, &t);
     if (s != HGAP_OK) return s;
+    uint32_t min_len = hgap::kMaxLen;
+    uint64_t kraft = 0;  // units of 2^-16; a complete book (sum 1) has no invalid table entry
+    for (uint32_t i = 0; i < book.symbol_count; ++i) {
+        if (book.symbols[i].length < min_len) min_len = book.symbols[i].length;
+        kraft += 1ull << (hgap::kMaxLen - book.symbols[i].length);
+    }
     hgap::DecArgs a;
     std::memset(&a, 0, sizeof(a));
     hgap::DecJob& J = a.single;
@@ -196,7 +202,7 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     J.out_aligned = reinterpret_cast<uint8_t*>(addr - J.out_lo);
     J.n = n;
     J.item0 = 0;
-    J.ntiles = hgap::decode_tiles(segments);
+    J.ntiles = hgap::decode_tiles(segments, min_len);
     if (J.ntiles >= 0xffffffffull) return HGAP_ERR_UNSUPPORTED;
     a.count = 1;
     a.nitems = J.ntiles;
@@ -208,12 +214,6 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     a.lookback = reinterpret_cast<uint64_t*>(ws + kWsHeader);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     if (cudaMemsetAsync(ws, 0, need, st) != cudaSuccess) return HGAP_ERR_CUDA;
-    uint32_t min_len = hgap::kMaxLen;
-    uint64_t kraft = 0;  // units of 2^-16; a complete book (sum 1) has no invalid table entry
-    for (uint32_t i = 0; i < book.symbol_count; ++i) {
-        if (book.symbols[i].length < min_len) min_len = book.symbols[i].length;
-        kraft += 1ull << (hgap::kMaxLen - book.symbols[i].length);
-    }
     const bool complete = kraft == (1ull << hgap::kMaxLen);
     // two symbols per lookup pay off once about a third of the lookups yield two
     const bool pairs = hgap::dec_pair_fraction(t) >= 0.3;

@@ -264,7 +264,8 @@ __global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count
         uint32_t c = kNoClass;
         if (j < count) {
             c = cls[j];
-            if (c != kNoClass) nt = (entries[j].segments + 511) / 512;
+            // tile size of the class's decoder: 256 segments for 1-bit shortest codes
+            if (c != kNoClass) nt = (entries[j].segments + (c / 2 == 3 ? 255 : 511)) / (c / 2 == 3 ? 256 : 512);
         }
         uint64_t total = 0;
         const uint64_t rec0 = carry + block_excl_scan_u64(nt, &total, s_warp);
@@ -430,8 +431,9 @@ DecLayout dec_layout(uint32_t count, size_t workspace_bytes) {
 }
 
 uint64_t worst_tiles(uint32_t count, const uint64_t* sizes) {
-    uint64_t cap = 0;  // a stream has at most ceil(n / 8) segments (16-bit codes): ceil(n / 4096) tiles
-    for (uint32_t j = 0; j < count; ++j) cap += (sizes[j] + 4095) / 4096;
+    // a stream has at most ceil(n / 8) segments (16-bit codes): ceil(n / 2048) tiles of 256
+    uint64_t cap = 0;
+    for (uint32_t j = 0; j < count; ++j) cap += (sizes[j] + 2047) / 2048;
     return cap;
 }
 

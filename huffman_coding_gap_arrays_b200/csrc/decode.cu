@@ -27,22 +27,27 @@
 namespace hgap {
 
 constexpr int kDecThreads = 256;
-constexpr int kDecSegs = 512;   // segments per tile: two per thread
+// Segments per tile: two per thread, except for books whose shortest code
+// has 1 bit (R = 32 stage rows), where one per thread halves the stage and
+// compact areas and lets two CTAs share an SM instead of one.
+__host__ __device__ constexpr int dec_tile_segs(int R) { return R == 32 ? 256 : 512; }
 constexpr int kDecLookK = 8;    // look-back window = 32 * 8 tiles
 
 template <int R>  // stage rows of 4 symbols per segment: at most 4R symbols per segment
 struct DecCfg {
     static constexpr int kMaxSym = 4 * R;
+    static constexpr int kSegs = dec_tile_segs(R);
+    static constexpr int kPer = kSegs / kDecThreads;   // segments per thread
     static constexpr int kWarps = kDecThreads / 32;
     static constexpr int kT1 = 1 << kDecPrefix;        // u32 level-1 entries
     static constexpr int kT2 = kDecT2Cap;              // u16 level-2 entries
-    static constexpr int kWords = 4 * kDecSegs + 8;    // bitstream words staged per tile
+    static constexpr int kWords = 4 * kSegs + 8;       // bitstream words staged per tile
     static constexpr int kWordsPad = (kWords + kWords / 8 + 8 + 3) & ~3;
     static constexpr int kWordsPer = (kWords + kDecThreads - 1) / kDecThreads;
-    static constexpr int kGapStage = kDecSegs / 8 + 4;  // gap words of the tile (+1 before)
-    static constexpr int kPitch = kDecSegs + 4;        // stage row pitch (bytes): rows skew banks
+    static constexpr int kGapStage = kSegs / 8 + 4;     // gap words of the tile (+1 before)
+    static constexpr int kPitch = kSegs + 4;           // stage row pitch (bytes): rows skew banks
     static constexpr int kStageBytes = kMaxSym * kPitch;
-    static constexpr int kCompactBytes = kDecSegs * kMaxSym + 64;
+    static constexpr int kCompactBytes = kSegs * kMaxSym + 64;
     static constexpr size_t kSmem = (size_t)(kT1 + kT2 / 2 + kWordsPad + kGapStage) * 4 +
                                     kStageBytes + kCompactBytes;
     static_assert(kT1 % 4 == 0 && (kT2 / 2) % 4 == 0 && kWordsPad % 4 == 0 && kGapStage % 4 == 0 &&
@@ -141,7 +146,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
     do {                                                                                      \
         const DecSlot& ps = slot[S];                                                          \
         const bool ok = ps.item < s_nitems;                                                   \
-        const uint64_t ps0 = ps.local * kDecSegs;                                             \
+        const uint64_t ps0 = ps.local * C::kSegs;                                             \
         _Pragma("unroll") for (int j = 0; j < C::kWordsPer; ++j) {                            \
             const uint32_t i = tid + j * kDecThreads;                                         \
             const uint64_t w = 4 * ps0 + i;                                                   \
@@ -187,7 +192,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
         const int ns = ti == 2 ? 0 : ti + 1;  // slot of the next tile
         uint32_t claim = 0;
         if (tid == 0 && have) claim = atomicAdd(a.counter, 1u);  // its latency hides behind the decode
-        const uint64_t s0 = T.local * kDecSegs;  // first segment of the tile within its job
+        const uint64_t s0 = T.local * C::kSegs;  // first segment of the tile within its job
         const uint64_t segments = T.job.segments;
         const uint64_t stream_bits = T.job.words * 32;
         auto gap_of = [&](uint64_t k) -> uint32_t {  // k in [s0 - 1, s0 + 512)
@@ -195,11 +200,11 @@ __global__ void __launch_bounds__(kDecThreads, 3)
             return (sg[j] >> (4 * (uint32_t)(k & 7))) & 0xfu;
         };
 
-        // ---- 1. decode segments tid and tid + 256, one after the other ---------
+        // ---- 1. decode segments tid (and tid + 256), one after the other -------
         uint32_t n[2] = {0, 0};
         if (have) {
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
+            for (int k = 0; k < C::kPer; ++k) {
                 const uint32_t col = tid + k * kDecThreads;
                 const uint64_t s = s0 + col;
                 uint32_t cnt = 0;
@@ -336,7 +341,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
         // ---- 4. compact this tile at tile-local offsets (alignment applied on write-out)
         if (have) {
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
+            for (int k = 0; k < C::kPer; ++k) {
                 const uint8_t* src = stage + tid + k * kDecThreads;
                 uint8_t* dst = compact + excl[k];
                 for (uint32_t j = 0; j < n[k]; ++j) dst[j] = src[j * C::kPitch];
@@ -354,7 +359,11 @@ __global__ void __launch_bounds__(kDecThreads, 3)
 #undef HGAP_COMMIT
 }
 
-uint64_t decode_tiles(uint64_t segments) { return (segments + kDecSegs - 1) / kDecSegs; }
+uint64_t decode_tiles(uint64_t segments, uint32_t min_len) {
+    const uint32_t max_sym = (128 + min_len - 1) / (min_len ? min_len : 1);
+    const uint64_t segs = max_sym > 64 ? dec_tile_segs(32) : dec_tile_segs(16);
+    return (segments + segs - 1) / segs;
+}
 
 template <int R, bool COMPLETE, bool PAIRS>
 static int launch_decode_r(const DecArgs& a, const DecTable& t, int ctas_per_sm, cudaStream_t st) {

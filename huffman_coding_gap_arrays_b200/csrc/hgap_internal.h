@@ -171,7 +171,9 @@ int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool co
 // rate under the code's own distribution, where every 11-bit prefix is
 // equally likely).
 double dec_pair_fraction(const DecTable& t);
-uint64_t decode_tiles(uint64_t segments);
+// Tiles of a stream for a book whose shortest code is min_len bits (the
+// decoder's tile size depends on it); min_len = 1 gives the most.
+uint64_t decode_tiles(uint64_t segments, uint32_t min_len);
 
 // ------------------------------------------------------------- host helpers -
 void make_enc_table(const hgap_codebook& cb, EncTable* t);

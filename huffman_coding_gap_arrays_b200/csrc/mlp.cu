@@ -145,12 +145,13 @@ __global__ void __launch_bounds__(kThreads) mlp_grad_kernel(const float* __restr
     }
 }
 
+// Adam on the gradient plus an L2 term (weight_decay * p).
 __global__ void mlp_adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
-                                float* __restrict__ v, float lr, float b1, float b2, float eps, float c1,
-                                float c2) {
+                                float* __restrict__ v, float lr, float b1, float b2, float eps, float wd,
+                                float c1, float c2) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kParams) return;
-    const float gi = g[i];
+    const float gi = fmaf(wd, p[i], g[i]);
     const float mi = b1 * m[i] + (1.f - b1) * gi;
     const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
     m[i] = mi;
@@ -193,12 +194,12 @@ hgap_status hgap_mlp_loss_grad(const float* d_params, const float* d_x, const fl
 }
 
 hgap_status hgap_mlp_adam(float* d_params, const float* d_grad, float* d_m, float* d_v, uint32_t step,
-                          float lr, float beta1, float beta2, float eps, hgap_stream_t stream) {
+                          float lr, float beta1, float beta2, float eps, float weight_decay, hgap_stream_t stream) {
     if (!d_params || !d_grad || !d_m || !d_v || step == 0) return HGAP_ERR_INVALID_ARG;
     const float c1 = 1.f - (float)std::pow((double)beta1, (double)step);
     const float c2 = 1.f - (float)std::pow((double)beta2, (double)step);
     mlp_adam_kernel<<<(kParams + 255) / 256, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-        d_params, d_grad, d_m, d_v, lr, beta1, beta2, eps, c1, c2);
+        d_params, d_grad, d_m, d_v, lr, beta1, beta2, eps, weight_decay, c1, c2);
     return cuda_status(cudaGetLastError());
 }
 

@@ -11,9 +11,9 @@ move with the launch shape.
 
 It is trained on the autotuner's own records (``tuner.Autotuner``).
 ``LearnedTuner.choose`` scores every candidate shape with a forward pass of an
-ensemble of networks (mean over seeds) and keeps the default shape unless a
-candidate is predicted to be faster by a margin -- the exhaustive autotuner's
-pick without its measurements.  It only chooses launch shapes, which leave the
+ensemble of networks (one per seed) and keeps the default shape unless a
+candidate that every network predicts faster has a mean predicted gain above
+a margin -- the exhaustive autotuner's pick without its measurements.  It only chooses launch shapes, which leave the
 output format unchanged.  Untrained, or with a held-out error above its
 limit, it falls back to running the autotuner.
 """
@@ -105,14 +105,17 @@ class LaunchMLP:
                                        _stream(stream)), "hgap_mlp_loss_grad")
         return self.loss, self.grad
 
-    def adam_step(self, lr: float, b1=0.9, b2=0.999, eps=1e-8, stream=None) -> None:
+    def adam_step(self, lr: float, b1=0.9, b2=0.999, eps=1e-8, weight_decay=0.0, stream=None) -> None:
         self.step += 1
         check(lib().hgap_mlp_adam(self.params.data_ptr(), self.grad.data_ptr(), self.m.data_ptr(),
-                                  self.v.data_ptr(), self.step, lr, b1, b2, eps, _stream(stream)), "hgap_mlp_adam")
+                                  self.v.data_ptr(), self.step, lr, b1, b2, eps, weight_decay, _stream(stream)),
+              "hgap_mlp_adam")
 
-    def fit(self, X, T, steps: int = 3000, lr: float = 3e-3, log_every: int = 0) -> list:
-        """Full-batch Adam on the mean squared error of the targets, with the
-        learning rate decaying tenfold over the run."""
+    def fit(self, X, T, steps: int = 3000, lr: float = 3e-3, weight_decay: float = 1e-3,
+            log_every: int = 0) -> list:
+        """Full-batch Adam on the mean squared error of the targets plus a small
+        L2 term (timings are noisy; cross-validation over recorded batches
+        picked 1e-3), with the learning rate decaying tenfold over the run."""
         X = np.asarray(X, np.float32)
         T = np.asarray(T, np.float32)
         self.mean = X.mean(0).astype(np.float32)
@@ -123,7 +126,7 @@ class LaunchMLP:
         losses = []
         for k in range(steps):
             self.loss_grad_normalized(Xn, Td, scale)
-            self.adam_step(lr * (0.1 ** (k / max(steps, 1))))
+            self.adam_step(lr * (0.1 ** (k / max(steps, 1))), weight_decay=weight_decay)
             if log_every and (k % log_every == 0 or k == steps - 1):
                 losses.append(float(self.loss.item()))
         if not losses:
@@ -170,11 +173,15 @@ class LearnedTuner:
         return bool(self.mlps) and self.holdout_rmse <= self.max_rmse
 
     def _pick(self, f, cands, default, out: int, margin: float):
+        """Among the candidates that every member of the ensemble predicts
+        faster than the default, the one with the best mean prediction --
+        taken only if that mean gain exceeds the margin."""
         X = np.stack([np.concatenate([f, config_vector(c)]) for c in list(cands) + [default]])
-        P = self.predict(X)[:, out]
-        i = int(np.argmin(P[:-1]))
-        # leave the default only for a predicted gain beyond the margin
-        return cands[i] if P[i] < P[-1] + math.log(1.0 - margin) else default
+        P = np.stack([m.predict(X)[:, out] for m in self.mlps])  # members x (candidates + default)
+        rel = P[:, :-1] - P[:, -1:]                               # log time relative to the default
+        mean = np.where((rel < 0).all(axis=0), rel.mean(axis=0), np.inf)
+        i = int(np.argmin(mean))
+        return cands[i] if mean[i] < math.log(1.0 - margin) else default
 
     def choose(self, features) -> LaunchConfig:
         """The compress shape with the least predicted compress time, then the

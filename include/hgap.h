@@ -267,7 +267,7 @@ hgap_status hgap_batch_status(const void* d_workspace, hgap_stream_t stream);
  * d_x: n x 8 inputs, d_y / d_target: n x 2 (NaN targets are unmeasured and
  * carry no loss).  loss = scale * sum (y - t)^2 / 2; hgap_mlp_loss_grad
  * overwrites d_grad (HGAP_MLP_PARAMS floats) and *d_loss.  Adam with bias
- * correction for step >= 1. */
+ * correction for step >= 1, on the gradient plus weight_decay * params. */
 #define HGAP_MLP_IN 8
 #define HGAP_MLP_HIDDEN 32
 #define HGAP_MLP_OUT 2
@@ -278,7 +278,8 @@ hgap_status hgap_mlp_forward(const float* d_params, const float* d_x, uint32_t n
 hgap_status hgap_mlp_loss_grad(const float* d_params, const float* d_x, const float* d_target, uint32_t n,
                                float scale, float* d_grad, float* d_loss, hgap_stream_t stream);
 hgap_status hgap_mlp_adam(float* d_params, const float* d_grad, float* d_m, float* d_v, uint32_t step,
-                          float lr, float beta1, float beta2, float eps, hgap_stream_t stream);
+                          float lr, float beta1, float beta2, float eps, float weight_decay,
+                          hgap_stream_t stream);
 
 /* ------------------------------------------------------------------ container
  * Writer encoder/src/huff.cpp:111-125, reader decoder/src/huff.cpp:27-81:

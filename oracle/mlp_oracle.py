@@ -60,7 +60,8 @@ def loss_grad(p, X, T, scale):
     return loss, pack(g)
 
 
-def adam(p, g, m, v, step, lr, b1=0.9, b2=0.999, eps=1e-8):
+def adam(p, g, m, v, step, lr, b1=0.9, b2=0.999, eps=1e-8, wd=0.0):
+    g = g + wd * p  # L2 term
     m = b1 * m + (1 - b1) * g
     v = b2 * v + (1 - b2) * g * g
     mh = m / (1 - b1 ** step)

@@ -154,7 +154,7 @@ def test_batch_host_queries():
     # regions: ceil((n + 15) / 64 KiB) per non-empty buffer
     regions = sum(int(-(-(int(n) + 15) // 65536)) for n in sizes if n)
     assert enc >= regions * (8 + 1024)
-    assert dec >= sum(int(-(-int(n) // 4096)) for n in sizes) * 40
+    assert dec >= sum(int(-(-int(n) // 2048)) for n in sizes) * 40
     cfg1 = BatchConfig(1, 0, 0, 0)
     assert L.hgap_batch_compress_workspace_bytes(sizes.size, p, C.byref(cfg1)) > enc
     # worst case 16 bits per byte, each bitstream rounded up to 16 bytes
