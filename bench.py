@@ -285,7 +285,8 @@ def train_learned_tuner(dev):
     from huffman_coding_gap_arrays_b200 import workloads as WL
     shapes = [(64, 64 << 10), (256, 256 << 10), (512, 1 << 20), (128, 4 << 20), (1024, 4 << 20),
               (2048, 1 << 20), (32, 16 << 20), (384, 2 << 20), (1536, 512 << 10), (768, 4 << 20),
-              (96, 8 << 20), (2048, 4 << 20)]
+              (96, 8 << 20), (2048, 4 << 20), (128, 128 << 10), (1024, 2 << 20), (3000, 4 << 20),
+              (48, 32 << 20), (640, 1 << 20), (2600, 2 << 20), (200, 16 << 20), (4096, 4 << 20)]
     hold = [(200, 2 << 20), (1200, 4 << 20)]
 
     def records(sh, seed):
@@ -294,7 +295,7 @@ def train_learned_tuner(dev):
             sz = WL.batch_sizes(count, lo=4096, hi=hi, seed=seed + k)
             bufs = [WL.batch_buffer(n, (seed + k) * 7919 + i, device=dev) for i, n in enumerate(sz)]
             outs = [torch.empty_like(b) for b in bufs]
-            recs.extend(T.Autotuner(reps=2, warmup=1).tune(bufs, outs, T.batch_features(bufs)).records)
+            recs.extend(T.Autotuner(reps=5, warmup=2).tune(bufs, outs, T.batch_features(bufs)).records)
             del bufs, outs
         return recs
 

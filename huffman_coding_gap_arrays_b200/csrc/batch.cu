@@ -210,9 +210,9 @@ __global__ void __launch_bounds__(kScanThreads) benc_place_kernel(uint32_t count
 
 // ------------------------------------------------------------- decompress ---
 
+// 8 classes: the decoder's stage size (from the shortest code) x complete book
 __device__ __forceinline__ uint32_t class_of(uint32_t min_len, bool complete) {
-    const uint32_t max_sym = (128 + min_len - 1) / min_len;
-    const uint32_t r = max_sym <= 32 ? 0 : max_sym <= 44 ? 1 : max_sym <= 64 ? 2 : 3;
+    const uint32_t r = min_len >= 4 ? 0 : 4 - min_len;  // stage rows 8, 11, 16, 32
     return 2 * r + (complete ? 1 : 0);
 }
 
@@ -264,8 +264,10 @@ __global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count
         uint32_t c = kNoClass;
         if (j < count) {
             c = cls[j];
-            // tile size of the class's decoder: 256 segments for 1-bit shortest codes
-            if (c != kNoClass) nt = (entries[j].segments + (c / 2 == 3 ? 255 : 511)) / (c / 2 == 3 ? 256 : 512);
+            if (c != kNoClass) {  // tiles of the class's decoder
+                const uint64_t segs = dec_tile_segs(dec_stage_rows(c / 2 == 0 ? 4 : 4 - c / 2));
+                nt = (entries[j].segments + segs - 1) / segs;
+            }
         }
         uint64_t total = 0;
         const uint64_t rec0 = carry + block_excl_scan_u64(nt, &total, s_warp);

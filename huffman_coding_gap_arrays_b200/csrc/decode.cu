@@ -27,10 +27,7 @@
 namespace hgap {
 
 constexpr int kDecThreads = 256;
-// Segments per tile: two per thread, except for books whose shortest code
-// has 1 bit (R = 32 stage rows), where one per thread halves the stage and
-// compact areas and lets two CTAs share an SM instead of one.
-__host__ __device__ constexpr int dec_tile_segs(int R) { return R == 32 ? 256 : 512; }
+// Segments per tile: dec_tile_segs(R) (hgap_internal.h).
 constexpr int kDecLookK = 8;    // look-back window = 32 * 8 tiles
 
 template <int R>  // stage rows of 4 symbols per segment: at most 4R symbols per segment
@@ -360,8 +357,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
 }
 
 uint64_t decode_tiles(uint64_t segments, uint32_t min_len) {
-    const uint32_t max_sym = (128 + min_len - 1) / (min_len ? min_len : 1);
-    const uint64_t segs = max_sym > 64 ? dec_tile_segs(32) : dec_tile_segs(16);
+    const uint64_t segs = dec_tile_segs(dec_stage_rows(min_len ? min_len : 1));
     return (segments + segs - 1) / segs;
 }
 
@@ -387,24 +383,24 @@ static int launch_decode_r(const DecArgs& a, const DecTable& t, int ctas_per_sm,
 }
 
 template <bool COMPLETE, bool PAIRS>
-static int launch_decode_c(const DecArgs& a, const DecTable& t, uint32_t max_sym, int k, cudaStream_t st) {
-    if (max_sym <= 32) return launch_decode_r<8, COMPLETE, PAIRS>(a, t, k, st);
-    if (max_sym <= 44) return launch_decode_r<11, COMPLETE, PAIRS>(a, t, k, st);
-    if (max_sym <= 64) return launch_decode_r<16, COMPLETE, PAIRS>(a, t, k, st);
-    return launch_decode_r<32, COMPLETE, PAIRS>(a, t, k, st);
+static int launch_decode_c(const DecArgs& a, const DecTable& t, uint32_t min_len, int k, cudaStream_t st) {
+    switch (dec_stage_rows(min_len)) {
+        case 8: return launch_decode_r<8, COMPLETE, PAIRS>(a, t, k, st);
+        case 11: return launch_decode_r<11, COMPLETE, PAIRS>(a, t, k, st);
+        case 16: return launch_decode_r<16, COMPLETE, PAIRS>(a, t, k, st);
+        default: return launch_decode_r<32, COMPLETE, PAIRS>(a, t, k, st);
+    }
 }
 
-// min_len: shortest code length of the book.  A segment holds at most
-// ceil(128 / min_len) codeword starts; the stage is sized for that.
 int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, bool pairs,
                   int ctas_per_sm, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const uint32_t max_sym = (128 + min_len - 1) / (min_len ? min_len : 1);
+    if (min_len == 0) min_len = 1;
     if (pairs)
-        return complete ? launch_decode_c<true, true>(a, t, max_sym, ctas_per_sm, st)
-                        : launch_decode_c<false, true>(a, t, max_sym, ctas_per_sm, st);
-    return complete ? launch_decode_c<true, false>(a, t, max_sym, ctas_per_sm, st)
-                    : launch_decode_c<false, false>(a, t, max_sym, ctas_per_sm, st);
+        return complete ? launch_decode_c<true, true>(a, t, min_len, ctas_per_sm, st)
+                        : launch_decode_c<false, true>(a, t, min_len, ctas_per_sm, st);
+    return complete ? launch_decode_c<true, false>(a, t, min_len, ctas_per_sm, st)
+                    : launch_decode_c<false, false>(a, t, min_len, ctas_per_sm, st);
 }
 
 }  // namespace hgap

@@ -6,6 +6,12 @@
 
 #include "../../include/hgap.h"
 
+#ifdef __CUDACC__
+#define HGAP_HD __host__ __device__
+#else
+#define HGAP_HD
+#endif
+
 namespace hgap {
 
 // ---------------------------------------------------------------- format ---
@@ -124,6 +130,17 @@ struct HistStArgs {
 //   pointer entry: bit15=1, bits 12..14 = extra width w, bits 0..11 = level-2 offset
 // Level 2 holds direct entries, 2^w per level-1 prefix whose codes are longer.
 constexpr int kDecPrefix = 11;
+// Decoder stage rows (of 4 symbols) for a book whose shortest code has
+// min_len bits: a 128-bit segment holds at most ceil(128 / min_len) symbols.
+HGAP_HD constexpr int dec_stage_rows(uint32_t min_len) {
+    return min_len >= 4 ? 8 : min_len == 3 ? 11 : min_len == 2 ? 16 : 32;
+}
+// Segments per decoder tile for a stage of R rows: two per thread, or one
+// per thread where the stage is large (R >= 16: it halves the stage and
+// compact areas so that more CTAs share an SM; measured 31 % faster for
+// R = 32, 3 % for R = 16, and 33 % slower for R = 11, where the per-tile
+// work then dominates).
+HGAP_HD constexpr int dec_tile_segs(int R) { return R >= 16 ? 256 : 512; }
 constexpr int kDecT2Cap = 2560;  // >= the largest complete 16-bit book (see host.cpp)
 constexpr uint16_t kDecInvalid = 0x4000;
 struct DecTable {
