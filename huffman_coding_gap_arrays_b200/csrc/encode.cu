@@ -124,10 +124,12 @@ __device__ __forceinline__ uint32_t st_chunks(const EncJob& J, uint64_t st) {
     return (uint32_t)((v1 - v0 + kEncChunkBytes - 1) / kEncChunkBytes);
 }
 
-// Thread 0's bulk-copy producer.  Copies go out in the order the CTA encodes
-// chunks: the rest of the current region, then the claimed next one; at most
-// kRing beyond the last chunk whose buffer is free again.  Its state lives in
-// shared memory (only thread 0 touches it), sparing every thread the registers.
+// The bulk-copy producer: thread 0 at region boundaries, the last warp's first
+// thread after each chunk's second barrier (never both at once; barriers order
+// them).  Copies go out in the order the CTA encodes chunks: the rest of the
+// current region, then the claimed next one; at most kRing beyond the last
+// chunk whose buffer is free again.  Its state lives in shared memory (one
+// thread touches it at a time), sparing every thread the registers.
 __device__ __forceinline__ void produce(const EncArgs& a, uint8_t* ring, EncShared& sh, uint32_t freed, int cur_slot) {
     uint32_t issued = sh.p_issued, pc = sh.p_chunk;
     int which = sh.p_which;
@@ -312,12 +314,8 @@ __global__ void __launch_bounds__(kEncThreads, 2)
             const uint32_t incl = warp_incl_scan(nbits, lane);
             if (lane == 31) sh.warp_tot[warp] = incl;
             __syncthreads();  // (1) warp totals visible; this ring buffer read; previous chunk written out
-            if (tid == 0) {
-                // the word carried in (previous chunk's tail, or the rebuilt head word)
-                if (sh.carry) atomicOr(img + ((P >> 5) & 3), sh.carry);
-                fence_proxy_async_smem();
-                produce(a, ring, sh, cons + 1, cur_slot);
-            }
+            // the word carried in (previous chunk's tail, or the rebuilt head word)
+            if (tid == 0 && sh.carry) atomicOr(img + ((P >> 5) & 3), sh.carry);
             uint32_t wt = lane < (uint32_t)kEncWarps ? sh.warp_tot[lane] : 0u;
             wt = warp_incl_scan(wt, lane);
             const uint32_t L = __shfl_sync(kFull, wt, kEncWarps - 1);
@@ -353,6 +351,12 @@ __global__ void __launch_bounds__(kEncThreads, 2)
                 if (nb) atomicOr(img + wi, cur_w);
             }
             __syncthreads();  // (2) image complete
+            // the last warp, whose write-out share is the smallest, refills the ring
+            // (this chunk's buffer was read before barrier (1))
+            if (tid == kEncThreads - 32) {
+                fence_proxy_async_smem();
+                produce(a, ring, sh, cons + 1, cur_slot);
+            }
 
             // write out complete words [P>>5, E>>5), clearing the image behind;
             // the group holding word E>>5 hands it on as the carry
