@@ -392,7 +392,8 @@ __global__ void __launch_bounds__(kEncThreads, 2)
             const uint64_t kb = P >> 7, kn = E >> 7;  // segments ending in this chunk: [kb, kn)
             const uint64_t kb8 = kb & ~7ull;
             const uint32_t nk = (uint32_t)(8 * ((kn >> 3) - (kb8 >> 3) + 1));
-            for (uint32_t t0 = warp * 32; t0 < nk; t0 += kEncThreads) {  // warp-uniform
+            // highest warps first: the write-out above took the lowest ones
+            for (uint32_t t0 = (kEncWarps - 1 - warp) * 32; t0 < nk; t0 += kEncThreads) {  // warp-uniform
                 const uint32_t t = t0 + lane;
                 const uint64_t k = kb8 + t;
                 uint32_t v = 0;
