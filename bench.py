@@ -330,14 +330,18 @@ def run_serving(args, pool, learned, fixed_cfg, dev):
     traffic = T.batch_features(bufs)[1:]
     out = {"requests": args.serve_requests, "offered_gbs": args.serve_gbs, "hbm_budget_gb": 40,
            "sizes": "log-uniform 64 KiB .. 64 MiB, 50/50 compress/decompress, Poisson arrivals",
+           "warmup": "an untimed stream of a fifth as many requests first, per policy",
            "where": "payloads and results resident in HBM; latency = queueing + GPU service"}
     policies = [("autotuner_fixed", dict(config=fixed_cfg))]
     if learned is not None and learned.usable:
         policies.insert(0, ("mlp", dict(tuner=learned)))
     policies.append(("plain", dict(policy="plain")))
     for name, kw in policies:
-        reqs = SV.poisson_requests(args.serve_requests, args.serve_gbs, pool, streams, seed=23)
         srv = SV.Server(hbm_budget=40e9, traffic_features=traffic, device=dev, **kw)
+        # untimed warm-up stream: the allocator's pools and the launch attributes settle first
+        srv.run(SV.poisson_requests(max(100, args.serve_requests // 5), args.serve_gbs, pool, streams, seed=29))
+        srv.batches, srv.peak_held = 0, 0
+        reqs = SV.poisson_requests(args.serve_requests, args.serve_gbs, pool, streams, seed=23)
         out[name] = srv.run(reqs)
         del reqs
         torch.cuda.synchronize()

@@ -42,6 +42,17 @@ def _u64p(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_uint64))
 
 
+def _upload(values, dtype, out: torch.Tensor | None = None, device=None) -> torch.Tensor:
+    """Host values to the device through pinned memory, ordered on the current
+    stream without blocking the host (a pageable copy would wait for the
+    stream's earlier work)."""
+    host = torch.as_tensor(np.asarray(values), dtype=dtype).pin_memory()
+    if out is None:
+        return host.to(device, non_blocking=True)
+    out.copy_(host, non_blocking=True)
+    return out
+
+
 class BatchCodec:
     """Workspaces, arenas and pointer tables for a fixed list of buffer sizes."""
 
@@ -63,7 +74,7 @@ class BatchCodec:
         self.bits = torch.empty(max(self.bits_capacity, 4), dtype=torch.int32, device=dev)
         self.gaps = torch.empty(max(self.gaps_capacity, 1), dtype=torch.int32, device=dev)
         self.entries = torch.zeros(max(self.count, 1) * ENTRY_BYTES, dtype=torch.uint8, device=dev)
-        self.d_sizes = torch.from_numpy(self.sizes.view(np.int64)).to(dev)
+        self.d_sizes = _upload(self.sizes.view(np.int64), torch.int64, device=dev)
         self.d_in = torch.zeros(max(self.count, 1), dtype=torch.int64, device=dev)
         self.d_out = torch.zeros(max(self.count, 1), dtype=torch.int64, device=dev)
         self.d_region = None
@@ -71,7 +82,7 @@ class BatchCodec:
             rc = np.asarray(region_chunks, np.uint8)
             if rc.size != self.count:
                 raise ValueError("one region size per buffer")
-            self.d_region = torch.from_numpy(rc.copy()).to(dev)
+            self.d_region = _upload(rc, torch.uint8, device=dev)
         self._inputs = self._outputs = None
 
     # ---------------------------------------------------------------- binding
@@ -80,11 +91,11 @@ class BatchCodec:
         uint8 CUDA tensors, one per size).  The tensors must stay alive."""
         if inputs is not None:
             self._check(inputs, "inputs")
-            self.d_in.copy_(torch.tensor([t.data_ptr() for t in inputs], dtype=torch.int64))
+            _upload([t.data_ptr() for t in inputs], torch.int64, out=self.d_in)
             self._inputs = list(inputs)
         if outputs is not None:
             self._check(outputs, "outputs")
-            self.d_out.copy_(torch.tensor([t.data_ptr() for t in outputs], dtype=torch.int64))
+            _upload([t.data_ptr() for t in outputs], torch.int64, out=self.d_out)
             self._outputs = list(outputs)
 
     def _check(self, bufs, name):

@@ -199,6 +199,40 @@ class LearnedTuner:
         self._memo[key] = pick
         return pick
 
+    def precompute(self, traffic, log2_lo: float, log2_hi: float) -> None:
+        """Fills the memo for every input size from 2^log2_lo to 2^log2_hi (in
+        the memo's 1/8 steps) for fixed byte statistics, with one forward pass
+        per network -- so that a serving loop never waits for one."""
+        keys = np.arange(np.floor(log2_lo * 8) / 8, np.ceil(log2_hi * 8) / 8 + 1e-9, 0.125)
+        if not len(keys) or not self.mlps:
+            return
+        d0 = self.default
+        comp = list(self.space)
+        base = LaunchConfig(d0.region_chunks, d0.hist_ctas_per_sm, d0.enc_ctas_per_sm, d0.dec_ctas_per_sm)
+        feats = [np.round(np.concatenate([[k], np.asarray(traffic, np.float32)]) * 8) / 8 for k in keys]
+        # stage 1: the compress shape for every size at once
+        X = np.stack([np.concatenate([f, config_vector(c)]) for f in feats for c in comp + [base]])
+        P = np.stack([m.predict(X)[:, 0] for m in self.mlps]).reshape(len(self.mlps), len(feats), len(comp) + 1)
+        picks = []
+        for j in range(len(feats)):
+            rel = P[:, j, :-1] - P[:, j, -1:]
+            mean = np.where((rel < 0).all(axis=0), rel.mean(axis=0), np.inf)
+            i = int(np.argmin(mean))
+            picks.append(comp[i] if mean[i] < math.log(1.0 - self.margin) else base)
+        # stage 2: the decoder grid for each size's compress shape
+        dec = [[LaunchConfig(c.region_chunks, c.hist_ctas_per_sm, c.enc_ctas_per_sm, d) for d in self.dec_space]
+               + [LaunchConfig(c.region_chunks, c.hist_ctas_per_sm, c.enc_ctas_per_sm, d0.dec_ctas_per_sm)]
+               for c in picks]
+        X = np.stack([np.concatenate([f, config_vector(c)]) for f, row in zip(feats, dec) for c in row])
+        nd = len(self.dec_space) + 1
+        P = np.stack([m.predict(X)[:, 1] for m in self.mlps]).reshape(len(self.mlps), len(feats), nd)
+        for j, f in enumerate(feats):
+            rel = P[:, j, :-1] - P[:, j, -1:]
+            mean = np.where((rel < 0).all(axis=0), rel.mean(axis=0), np.inf)
+            i = int(np.argmin(mean))
+            self._memo[tuple(f.astype(np.float32).tolist())] = (
+                dec[j][i] if mean[i] < math.log(1.0 - self.dec_margin) else dec[j][-1])
+
     def choose_or_search(self, features, inputs, outputs) -> LaunchConfig:
         """The ensemble's pick when it is trained and accurate enough on
         held-out records; otherwise the exhaustive autotuner on these buffers."""

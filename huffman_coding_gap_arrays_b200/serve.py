@@ -33,7 +33,7 @@ import torch
 
 from . import codec
 from ._lib import BatchEntry, check, lib
-from .batch import ENTRY_BYTES, BatchCodec, LaunchConfig
+from .batch import ENTRY_BYTES, BatchCodec, LaunchConfig, _upload
 from .codec import _stream
 
 
@@ -89,7 +89,8 @@ class Server:
 
     def __init__(self, policy: str = "batched", tuner=None, config: LaunchConfig | None = None,
                  hbm_budget: float = 40e9, max_batch: int = 64, max_inflight: int = 3,
-                 traffic_features=(5.0, 12.0, 0.05), device="cuda", keep_results: bool = False):
+                 traffic_features=(5.0, 12.0, 0.05), device="cuda", keep_results: bool = False,
+                 reserve_bytes: int = 4 << 30):
         if policy not in ("batched", "plain"):
             raise ValueError("policy is 'batched' or 'plain'")
         self.policy = policy
@@ -102,6 +103,15 @@ class Server:
         self.device = torch.device(device)
         self.keep_results = keep_results
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.max_inflight)]
+        self.free_streams = list(self.streams)  # a new batch only goes to a stream with nothing queued
+        if reserve_bytes and self.policy == "batched":
+            # one large cached block up front: per-batch allocations of varying size are
+            # then carved from it instead of each new size reaching the driver mid-run
+            for s_ in self.streams:
+                with torch.cuda.stream(s_):
+                    blk = torch.empty(int(reserve_bytes) // len(self.streams), dtype=torch.uint8,
+                                      device=self.device)
+                    del blk
         self.held = 0
         self.peak_held = 0
         self.batches = 0
@@ -126,7 +136,7 @@ class Server:
 
     # -------------------------------------------------------------- batches
     def _launch(self, reqs, t0) -> _Batch:
-        s = self.streams[self.batches % len(self.streams)]
+        s = self.free_streams.pop()
         self.batches += 1
         now = time.perf_counter() - t0
         for r in reqs:
@@ -165,9 +175,8 @@ class Server:
             C.memmove(C.byref(arr[i]), C.byref(r.stream.entry), ENTRY_BYTES)
             arr[i].bits_offset = (r.stream.bits.data_ptr() - base_b) // 4
             arr[i].gaps_offset = (r.stream.gaps.data_ptr() - base_g) // 4
-        host = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8)
-        d_ent = host.to(self.device, non_blocking=False)
-        d_out = torch.tensor([o.data_ptr() for o in outs], dtype=torch.int64).to(self.device)
+        d_ent = _upload(np.frombuffer(bytes(arr), np.uint8), torch.uint8, device=self.device)
+        d_out = _upload([o.data_ptr() for o in outs], torch.int64, device=self.device)
         sizes = np.array([r.nbytes for r in reqs], np.uint64)
         nbytes = lib().hgap_batch_decompress_workspace_bytes(count, sizes.ctypes.data_as(C.POINTER(C.c_uint64)))
         ws = torch.empty((nbytes + 7) // 8, dtype=torch.int64, device=self.device)
@@ -186,6 +195,7 @@ class Server:
             check(lib().hgap_batch_status(b.dec_ws.data_ptr(), _stream(b.stream)), "served decompress")
         for r in b.reqs:
             r.done = now
+        self.free_streams.append(b.stream)
         if b.plan is not None:
             comp = [r for r in b.reqs if r.kind == "compress"]
             raw = b.entries_host.numpy().tobytes()
@@ -208,6 +218,11 @@ class Server:
         reqs = sorted(requests, key=lambda r: r.arrival)
         if self.policy == "plain":
             return self._run_plain(reqs)
+        if self.tuner is not None and hasattr(self.tuner, "precompute"):
+            # every batch size the run can form, decided before the clock starts
+            sizes = [r.nbytes for r in reqs]
+            self.tuner.precompute(self.traffic, np.log2(max(1, min(sizes))),
+                                  np.log2(max(1, sum(sorted(sizes)[-self.max_batch:]))))
         pending = deque(reqs)
         queue = deque()
         inflight = []
