@@ -4,18 +4,21 @@
 // parallelism -- a 128-bit segment that starts at its gap offset -- but each
 // segment is decoded ONCE (the reference decodes it twice: a counting pass,
 // then a writing pass, decoder.cu:529-569,672-725):
-//   1. a persistent CTA of 256 threads takes the next tile of 512 segments,
-//      stages its bitstream words in shared memory (padded one word in eight
-//      so the threads' windows, 4 words apart, fall in different banks) and
-//      every thread decodes TWO segments interleaved (two independent
-//      dependency chains) through a shared-memory two-level table, parking the
-//      symbols in a column-major shared area sized for the book's shortest
-//      code (a segment holds at most ceil(128 / shortest length) symbols);
+//   1. a persistent CTA of 256 threads takes the next tile of 512 segments
+//      (256 for books with 1-2 bit codes), stages its bitstream words in
+//      shared memory (padded one word in eight so the threads' windows, 4
+//      words apart, fall in different banks) and every thread decodes its
+//      segments one after the other (interleaving two chains measured slower:
+//      the loop is issue-bound) through a shared-memory two-level table,
+//      parking each segment's symbols in its own shared row sized for the
+//      book's shortest code (a segment holds at most ceil(128 / shortest
+//      length) symbols);
 //   2. block scan of the 512 symbol counts + one bounded decoupled look-back
 //      with a 64-tile window gives the tile's output offset;
-//   3. the symbols are compacted into a shared image of the output at its
-//      16-byte alignment and written with 16-byte coalesced stores (byte
-//      stores only on the two ragged edges), clipped at exactly n bytes (the
+//   3. the rows are compacted (whole words where the destination is aligned)
+//      into a shared image of the tile's output and written one tile later,
+//      once its offset is known, with 16-byte coalesced stores (byte stores
+//      only on the two ragged edges), clipped at exactly n bytes (the
 //      reference writes past n, decoder.cu:529).
 // Checks: every segment must end exactly where the next gap entry says the
 // next segment starts, every codeword must exist, and the stream must yield at
@@ -46,8 +49,11 @@ struct DecCfg {
     static constexpr int kWordsPad = (kWords + kWords / 8 + 8 + 3) & ~3;
     static constexpr int kWordsPer = (kWords + kDecThreads - 1) / kDecThreads;
     static constexpr int kGapStage = kSegs / 8 + 4;     // gap words of the tile (+1 before)
-    static constexpr int kPitch = kSegs + 4;           // stage row pitch (bytes): rows skew banks
-    static constexpr int kStageBytes = kMaxSym * kPitch;
+    // stage row of one segment (bytes): its symbols, at least 4 bytes of slack for the
+    // unconditional second store of a pair, and an odd number of words so that
+    // the 32 rows a warp writes start in 32 different banks
+    static constexpr int kRow = ((kMaxSym + 4) / 4 | 1) * 4;
+    static constexpr int kStageBytes = kSegs * kRow + 16;
     static constexpr int kCompactBytes = kSegs * kMaxSym + 64;
     static constexpr size_t kSmem = (size_t)(kT1 + kT2 / 2 + kWordsPad + kGapStage) * 4 +
                                     kStageBytes + kCompactBytes;
@@ -215,13 +221,33 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                     uint32_t end = 128 * col + 128;
                     if (last && stream_bits - 128 * s0 < end) end = (uint32_t)(stream_bits - 128 * s0);
                     bool bad = false;
-                    uint8_t* out = stage + col;
+                    uint8_t* const row = stage + col * C::kRow;
+                    uint8_t* out = row;
                     // the window's two stream words live in registers; a code moves
                     // the position by at most 16 bits, so at most one new word per code
                     uint32_t w = pos >> 5;
                     uint32_t cw = sw[pidx(w)], nw = sw[pidx(w + 1)];
                     // every codeword is at least the book's shortest length, so a
                     // segment yields at most kMaxSym symbols: no count test needed
+                    if (PAIRS) {
+                        // while 11 bits remain, both codes of a pair entry start inside
+                        // the segment: the second symbol is stored unconditionally (a
+                        // single entry's is overwritten or lies past the count)
+                        const int end_pair = (int)end - kDecPrefix;
+                        while ((int)pos <= end_pair) {
+                            const uint32_t e = lookup(t1, t2, __funnelshift_l(nw, cw, pos));
+                            if (!COMPLETE && (e & 0x40000000u)) break;
+                            out[0] = (uint8_t)e;
+                            out[1] = (uint8_t)(e >> 8);
+                            out += 1 + ((e >> 16) & 1u);
+                            pos += e >> 24;
+                            if ((pos >> 5) != w) {
+                                ++w;
+                                cw = nw;
+                                nw = sw[pidx(w + 1)];
+                            }
+                        }
+                    }
                     while (pos < end) {
                         const uint32_t e = lookup(t1, t2, __funnelshift_l(nw, cw, pos));
                         if (!COMPLETE && (e & 0x40000000u)) {
@@ -235,12 +261,11 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                             const uint32_t l1 = pair ? ((e >> 17) & 15u) : tot;
                             const bool two = pair && pos + l1 < end;
                             out[0] = (uint8_t)e;
-                            if (two) out[C::kPitch] = (uint8_t)(e >> 8);
-                            out += two ? 2 * C::kPitch : C::kPitch;
+                            if (two) out[1] = (uint8_t)(e >> 8);
+                            out += two ? 2 : 1;
                             pos += two ? tot : l1;
                         } else {
-                            *out = (uint8_t)e;
-                            out += C::kPitch;
+                            *out++ = (uint8_t)e;
                             pos += e >> 24;
                         }
                         if ((pos >> 5) != w) {
@@ -249,7 +274,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                             nw = sw[pidx(w + 1)];
                         }
                     }
-                    cnt = (uint32_t)(out - (stage + col)) / C::kPitch;
+                    cnt = (uint32_t)(out - row);
                     if (!last && !bad && pos != 128 * col + 128 + gap_of(s)) bad = true;
                     if (bad) atomicOr(a.status, kDevCorrupt);
                 }
@@ -343,9 +368,24 @@ __global__ void __launch_bounds__(kDecThreads, 3)
         if (have) {
 #pragma unroll
             for (int k = 0; k < C::kPer; ++k) {
-                const uint8_t* src = stage + tid + k * kDecThreads;
-                uint8_t* dst = compact + excl[k];
-                for (uint32_t j = 0; j < n[k]; ++j) dst[j] = src[j * C::kPitch];
+                // bytes up to the next word boundary of `compact` one by one, then whole
+                // words (two source words funnel-shifted), then the last bytes
+                const uint8_t* src = stage + (tid + k * kDecThreads) * C::kRow;
+                const uint32_t d = excl[k], m = n[k];
+                uint32_t h = (4u - (d & 3u)) & 3u;
+                if (h > m) h = m;
+                for (uint32_t j = 0; j < h; ++j) compact[d + j] = src[j];
+                const uint32_t nwords = (m - h) >> 2;
+                const uint32_t* sw32 = reinterpret_cast<const uint32_t*>(src);
+                uint32_t* dw = reinterpret_cast<uint32_t*>(compact + d + h);
+                const uint32_t sh = 8 * h;
+                uint32_t lo = sw32[0];
+                for (uint32_t j = 0; j < nwords; ++j) {
+                    const uint32_t hi = sw32[j + 1];
+                    dw[j] = __funnelshift_r(lo, hi, sh);
+                    lo = hi;
+                }
+                for (uint32_t j = h + 4 * nwords; j < m; ++j) compact[d + j] = src[j];
             }
         }
         if (have_next) {  // sw/sg and the tables are no longer read for this tile
