@@ -15,6 +15,8 @@
 //   1. bdec_book    one warp per buffer: checks the book, builds its decoder
 //                   table, and puts the buffer in one of 8 classes (decoder
 //                   stage size by the shortest code x complete book or not);
+//      bdec_widen   one CTA per buffer: the decoder table in the widened form
+//                   the decode kernel keeps in shared memory (DecTableW);
 //   2. bdec_setup   one CTA: tiles per buffer, look-back record numbering,
 //                   and per class the numbering of the class's tiles;
 //   3. bdec_map     tile -> buffer map of each class;
@@ -27,6 +29,7 @@
 #include <cstring>
 
 #include "book.cuh"
+#include "dec_entry.cuh"
 
 namespace hgap {
 namespace {
@@ -211,6 +214,7 @@ __global__ void __launch_bounds__(kScanThreads) benc_place_kernel(uint32_t count
 // ------------------------------------------------------------- decompress ---
 
 // 8 classes: the decoder's stage size (from the shortest code) x complete book
+__constant__ int kStageRows[4] = {8, 11, 16, 32};
 __device__ __forceinline__ uint32_t class_of(uint32_t min_len, bool complete) {
     const uint32_t r = min_len >= 4 ? 0 : 4 - min_len;  // stage rows 8, 11, 16, 32
     return 2 * r + (complete ? 1 : 0);
@@ -247,6 +251,19 @@ __global__ void __launch_bounds__(32 * kBookWarps) bdec_book_kernel(uint32_t cou
             cls[j] = (uint8_t)c;
         }
         __syncwarp();
+    }
+}
+
+constexpr int kWidenThreads = 256;
+
+__global__ void __launch_bounds__(kWidenThreads) bdec_widen_kernel(uint32_t count, const DecTable* tables,
+                                                                   const uint8_t* cls, DecTableW* wtables) {
+    __shared__ __align__(16) uint16_t s1[1 << kDecPrefix];
+    __shared__ uint32_t s_used;
+    for (uint32_t j = blockIdx.x; j < count; j += gridDim.x) {
+        const uint32_t c = cls[j];
+        if (c == kNoClass) continue;  // uniform over the CTA
+        widen_tables(tables[j], dec_multi(kStageRows[c >> 1], (c & 1u) != 0), wtables[j], s1, &s_used);
     }
 }
 
@@ -362,6 +379,11 @@ unsigned book_grid(uint32_t count) {
     return (unsigned)(want < cap ? (want ? want : 1) : cap);
 }
 
+unsigned widen_grid(uint32_t count) {
+    const uint64_t cap = (uint64_t)sm_count() * 8;
+    return (unsigned)(count < cap ? (count ? count : 1) : cap);
+}
+
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 uint32_t base_chunks(const hgap_batch_config* cfg) {
@@ -405,12 +427,12 @@ uint64_t worst_regions(uint32_t count, const uint64_t* sizes, const hgap_batch_c
 }
 
 // Decompress workspace: [header 1024: status @0, counters[8] @64, class nitems[8] @128]
-// [jobs] [tables] [classes] [item0s 8 x (count+1)] then the per-tile arrays
+// [jobs] [tables] [widened tables] [classes] [item0s 8 x (count+1)] then the per-tile arrays
 // [records | job_of 8 x cap] for as many tiles as the rest holds.
 constexpr size_t kDecPerTile = 8 + 4 * kClasses;
 
 struct DecLayout {
-    size_t jobs, tables, cls, item0s, records, job_of, fixed;
+    size_t jobs, tables, wtables, cls, item0s, records, job_of, fixed;
     uint64_t tiles_cap;
 };
 
@@ -421,6 +443,8 @@ DecLayout dec_layout(uint32_t count, size_t workspace_bytes) {
     off = align256(off + sizeof(DecJob) * (size_t)count);
     L.tables = off;
     off = align256(off + sizeof(DecTable) * (size_t)count);
+    L.wtables = off;
+    off = align256(off + sizeof(DecTableW) * (size_t)count);
     L.cls = off;
     off = align256(off + (size_t)count);
     L.item0s = off;
@@ -575,6 +599,7 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     uint64_t* class_nitems = reinterpret_cast<uint64_t*>(ws + 128);
     DecJob* jobs = reinterpret_cast<DecJob*>(ws + L.jobs);
     DecTable* tables = reinterpret_cast<DecTable*>(ws + L.tables);
+    DecTableW* wtables = reinterpret_cast<DecTableW*>(ws + L.wtables);
     uint8_t* cls = ws + L.cls;
     uint64_t* item0s = reinterpret_cast<uint64_t*>(ws + L.item0s);
     uint64_t* records = reinterpret_cast<uint64_t*>(ws + L.records);
@@ -583,6 +608,8 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     if (cudaMemsetAsync(ws, 0, 1024, st) != cudaSuccess) return HGAP_ERR_CUDA;
     if (set_book_smem(bdec_book_kernel) != cudaSuccess) return HGAP_ERR_CUDA;
     bdec_book_kernel<<<book_grid(count), 32 * kBookWarps, kBookSmem, st>>>(count, d_entries, tables, cls, status);
+    if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
+    bdec_widen_kernel<<<widen_grid(count), kWidenThreads, 0, st>>>(count, tables, cls, wtables);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
     bdec_setup_kernel<<<1, kScanThreads, 0, st>>>(count, d_entries, cls, d_bits, d_gaps, d_outputs, jobs, item0s,
                                                   class_nitems, L.tiles_cap, status);
@@ -600,7 +627,7 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
         a.jobs = jobs;
         a.job_of = job_of + (uint64_t)c * L.tiles_cap;
         a.item0s = item0s + (uint64_t)c * (count + 1);
-        a.tables = tables;
+        a.tables = wtables;
         a.count = count;
         a.nitems_dev = class_nitems + c;
         a.lookback = records;

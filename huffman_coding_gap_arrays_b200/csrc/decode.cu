@@ -25,6 +25,7 @@
 // least n symbols; failures set kDevCorrupt / kDevSize, never trap.
 #include <cuda_runtime.h>
 
+#include "dec_entry.cuh"
 #include "device_util.cuh"
 
 namespace hgap {
@@ -56,36 +57,10 @@ struct DecCfg {
     static constexpr int kStageBytes = kSegs * kRow + 16;
     static constexpr int kCompactBytes = kSegs * kMaxSym + 64;
     static constexpr size_t kSmem = (size_t)(kT1 + kT2 / 2 + kWordsPad + kGapStage) * 4 +
-                                    kStageBytes + kCompactBytes;
+                                    kStageBytes + kCompactBytes + kT1;  // + first-code lengths (u8)
     static_assert(kT1 % 4 == 0 && (kT2 / 2) % 4 == 0 && kWordsPad % 4 == 0 && kGapStage % 4 == 0 &&
                   kStageBytes % 16 == 0, "16-byte aligned areas");
 };
-
-// Table entry in shared memory (u32): direct = len << 24 | symbol;
-// pointer = bit 31 | extra width << 16 | level-2 offset; invalid = bit 30;
-// pair (level 1 only, see widen_pair) = two symbols with bit 16 set.
-__device__ __forceinline__ uint32_t widen_entry(uint32_t e) {
-    if (e & 0x8000u) return 0x80000000u | (((e >> 12) & 7u) << 16) | (e & 0xfffu);
-    if (e & kDecInvalid) return 0x40000000u;
-    return ((((e >> 8) & 15u) + 1u) << 24) | (e & 0xffu);
-}
-
-// Level-1 entry in shared memory for prefix x, from the u16 table: when the
-// first code leaves room for a whole second code inside the same 11-bit
-// window, both are returned at once (a pair entry: symbol 1 | symbol 2 << 8 |
-// bit 16 | length 1 << 17 | total length << 24).  The second code is known
-// from the bits after the first alone, because it ends inside the window.
-__device__ __forceinline__ uint32_t widen_pair(const uint16_t* t1src, uint32_t x) {
-    const uint32_t e = widen_entry(t1src[x]);
-    if (e & 0xC0000000u) return e;  // pointer or invalid
-    const uint32_t l1 = e >> 24;
-    if (l1 >= (uint32_t)kDecPrefix) return e;
-    const uint32_t e2 = widen_entry(t1src[(x << l1) & ((1u << kDecPrefix) - 1u)]);
-    if (e2 & 0xC0000000u) return e;
-    const uint32_t l2 = e2 >> 24;
-    if (l1 + l2 > (uint32_t)kDecPrefix) return e;
-    return (e & 0xffu) | ((e2 & 0xffu) << 8) | 0x10000u | (l1 << 17) | ((l1 + l2) << 24);
-}
 
 __device__ __forceinline__ uint32_t pidx(uint32_t w) { return w + (w >> 3); }
 
@@ -112,7 +87,8 @@ struct DecSlot {
 // COMPLETE: the book's Kraft sum is 1 (every package-merge book with two or
 // more symbols), so no table entry is invalid and the decode loop skips that test.
 // PAIRS: level-1 entries carry two symbols where both codes fit in the window
-// (worth it for short-code books; for long codes the extra selects only cost).
+// (worth it for short-code books; for long codes the extra selects only cost);
+// with a complete book, up to three (multi entries, widen_multi).
 template <int R, bool COMPLETE, bool PAIRS>
 __global__ void __launch_bounds__(kDecThreads, 3)
     decode_kernel(const __grid_constant__ DecArgs a, const __grid_constant__ DecTable tab) {
@@ -124,16 +100,38 @@ __global__ void __launch_bounds__(kDecThreads, 3)
     uint32_t* sg = sw + C::kWordsPad;                    // gap words: sg[j] = gaps[s0/8 - 1 + j]
     uint8_t* stage = reinterpret_cast<uint8_t*>(sg + C::kGapStage);
     uint8_t* compact = stage + C::kStageBytes;
+    uint8_t* l1t = compact + C::kCompactBytes;            // multi entries: length of the first code
     __shared__ uint32_t warp_tot[C::kWarps];
     __shared__ DecSlot slot[3];  // ring: the tile being decoded, the next one, the previous one
     __shared__ uint64_t s_O;
     __shared__ uint64_t s_nitems;
     __shared__ uint32_t s_lut_job;
 
+    constexpr bool MULTI = PAIRS && dec_multi(R, COMPLETE);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // single path: the u16 tables widened here, once per CTA
     auto load_tables = [&](const DecTable& t) {
-        for (int i = tid; i < C::kT1; i += kDecThreads) t1[i] = PAIRS ? widen_pair(t.t1, i) : widen_entry(t.t1[i]);
+        for (int i = tid; i < C::kT1; i += kDecThreads) {
+            if (MULTI) {
+                t1[i] = widen_multi(t.t1, i);
+                l1t[i] = first_len(t.t1, i);
+            } else {
+                t1[i] = PAIRS ? widen_pair(t.t1, i) : widen_entry(t.t1[i]);
+            }
+        }
         for (int i = tid; i < C::kT2; i += kDecThreads) t2[i] = t.t2[i];
+    };
+    // batched path (always PAIRS): the buffer's tables come widened, copied in 16-byte groups
+    auto copy_tables = [&](const DecTableW& t) {
+        const uint4* s1 = reinterpret_cast<const uint4*>(t.t1);
+        for (int i = tid; i < C::kT1 / 4; i += kDecThreads) reinterpret_cast<uint4*>(t1)[i] = s1[i];
+        if (MULTI) {
+            const uint4* sl = reinterpret_cast<const uint4*>(t.l1);
+            for (int i = tid; i < C::kT1 / 16; i += kDecThreads) reinterpret_cast<uint4*>(l1t)[i] = sl[i];
+        }
+        const uint32_t g = t.t2_groups;
+        const uint4* s2 = reinterpret_cast<const uint4*>(t.t2);
+        for (uint32_t i = tid; i < g; i += kDecThreads) reinterpret_cast<uint4*>(t2)[i] = s2[i];
     };
     // thread 0: the tile `item` and its job into slot s
     auto fill_slot = [&](int s, uint64_t item) {
@@ -180,7 +178,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
         s_lut_job = a.jobs ? ~0u : 0u;
     }
     __syncthreads();
-    if (a.jobs && slot[0].item < s_nitems) load_tables(a.tables[slot[0].job_id]);
+    if (a.jobs && slot[0].item < s_nitems) copy_tables(a.tables[slot[0].job_id]);
     uint32_t pre[C::kWordsPer];
     uint32_t pre_gap = 0;
     HGAP_PREFETCH(0);
@@ -229,7 +227,48 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                     uint32_t cw = sw[pidx(w)], nw = sw[pidx(w + 1)];
                     // every codeword is at least the book's shortest length, so a
                     // segment yields at most kMaxSym symbols: no count test needed
-                    if (PAIRS) {
+                    if (MULTI) {
+                        // while 11 bits remain, every code of a multi entry starts inside
+                        // the segment: all three symbol bytes are stored unconditionally
+                        // (those past the entry's count are overwritten or lie past the
+                        // segment's count)
+                        const int end_multi = (int)end - kDecPrefix;
+                        while ((int)pos <= end_multi) {
+                            const uint32_t e = lookup(t1, t2, __funnelshift_l(nw, cw, pos));
+                            out[0] = (uint8_t)e;
+                            out[1] = (uint8_t)(e >> 8);
+                            out[2] = (uint8_t)(e >> 16);
+                            out += 1 + ((e >> 29) & 3u);
+                            pos += (e >> 24) & 31u;
+                            if ((pos >> 5) != w) {
+                                ++w;
+                                cw = nw;
+                                nw = sw[pidx(w + 1)];
+                            }
+                        }
+                        // the last bits: a whole entry while it ends inside the segment
+                        // (then every code in it starts there), else its first code alone
+                        while (pos < end) {
+                            const uint32_t x = __funnelshift_l(nw, cw, pos);
+                            const uint32_t e = lookup(t1, t2, x);
+                            const uint32_t tot = (e >> 24) & 31u, more = (e >> 29) & 3u;
+                            out[0] = (uint8_t)e;
+                            out[1] = (uint8_t)(e >> 8);
+                            out[2] = (uint8_t)(e >> 16);
+                            if (pos + tot <= end) {
+                                out += 1 + more;
+                                pos += tot;
+                            } else {
+                                out += 1;
+                                pos += more ? (uint32_t)l1t[x >> (32 - kDecPrefix)] : tot;
+                            }
+                            if ((pos >> 5) != w) {
+                                ++w;
+                                cw = nw;
+                                nw = sw[pidx(w + 1)];
+                            }
+                        }
+                    } else if (PAIRS) {
                         // while 11 bits remain, both codes of a pair entry start inside
                         // the segment: the second symbol is stored unconditionally (a
                         // single entry's is overwritten or lies past the count)
@@ -248,7 +287,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                             }
                         }
                     }
-                    while (pos < end) {
+                    while (!MULTI && pos < end) {
                         const uint32_t e = lookup(t1, t2, __funnelshift_l(nw, cw, pos));
                         if (!COMPLETE && (e & 0x40000000u)) {
                             bad = !last;  // zero padding after the final codeword may not decode
@@ -389,7 +428,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
             }
         }
         if (have_next) {  // sw/sg and the tables are no longer read for this tile
-            if (a.jobs && N.job_id != s_lut_job) load_tables(a.tables[N.job_id]);
+            if (a.jobs && N.job_id != s_lut_job) copy_tables(a.tables[N.job_id]);
             HGAP_COMMIT();
         }
         prev_s = have ? ti : -1;

@@ -148,6 +148,28 @@ struct DecTable {
     uint16_t t2[kDecT2Cap];
 };
 
+// Multi entries (up to three symbols per level-1 lookup) pay for their wider
+// stores and tail test only where codes are very short: complete books whose
+// stage has at least this many rows (32: a shortest code of 1 bit).  Measured
+// per 256 MiB: 2.2 bits/byte 0.518 -> 0.484 ms; from 16 rows on, Zipf(1.2)
+// (shortest code 2 bits) 0.699 -> 0.722 ms.
+constexpr int kDecMultiMinRows = 32;
+HGAP_HD constexpr bool dec_multi(int rows, bool complete) { return complete && rows >= kDecMultiMinRows; }
+
+// The decode kernel's shared-memory tables in their widened form (u32 level-1
+// entries: pair form, or multi form for a complete book, with the length of
+// the first code per prefix), built once per buffer on the batched path so
+// that a CTA moving to another buffer's tile copies them with 16-byte loads
+// instead of re-deriving every entry.  Only the level-2 groups in use travel.
+struct DecTableW {
+    uint32_t t1[1 << kDecPrefix];
+    uint8_t l1[1 << kDecPrefix];
+    uint16_t t2[kDecT2Cap];
+    uint32_t t2_groups;  // 16-byte groups of t2 in use
+    uint32_t pad[3];
+};
+static_assert(sizeof(DecTableW) % 16 == 0, "16-byte copies");
+
 // One stream to decode (same single / batched scheme as EncJob).  Its tiles
 // use look-back records [item0, item0 + ntiles).
 struct DecJob {
@@ -168,7 +190,7 @@ struct DecArgs {
     const DecJob* jobs;         // batched: [count]
     const uint32_t* job_of;     // batched: [nitems] job of each tile of this launch
     const uint64_t* item0s;     // batched: [count] first tile of each job in this launch's numbering
-    const DecTable* tables;     // batched: [count]
+    const DecTableW* tables;    // batched: [count]
     uint32_t count;
     uint64_t nitems;            // tiles in this launch
     const uint64_t* nitems_dev; // batched: the tile count in device memory (overrides nitems)

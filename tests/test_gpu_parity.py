@@ -29,6 +29,8 @@ def make(dist: str, n: int, seed: int) -> np.ndarray:
         return rng.integers(0, 2, size=n, dtype=np.uint8)
     if dist == "single":
         return np.full(n, 77, np.uint8)
+    if dist == "narrow":  # quantised N(128, 0.6): a 1-bit shortest code, up to three codes per lookup
+        return np.clip(np.round(128 + 0.6 * rng.standard_normal(n)), 0, 255).astype(np.uint8)
     if dist == "deep":  # Fibonacci-like skew -> codes up to the 16-bit limit
         p = 1.0 / 1.618 ** np.arange(40); p /= p.sum()
         x = rng.choice(40, size=n, p=p).astype(np.uint8)
@@ -64,7 +66,7 @@ def test_histogram_skewed_and_empty(cuda):
     assert int(H.histogram(empty).sum()) == 0
 
 
-@pytest.mark.parametrize("dist", ["zipf", "uniform", "two", "deep", "single"])
+@pytest.mark.parametrize("dist", ["zipf", "uniform", "two", "deep", "single", "narrow"])
 @pytest.mark.parametrize("n", SIZES)
 def test_encode_decode_match_oracle(cuda, dist, n):
     x = make(dist, n, 1000 + n)
