@@ -17,13 +17,14 @@ bin/decoder minus file I/O.  All inputs exceed the 126 MB L2, so no flush is
 needed between steps.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-    torchrun --nproc-per-node N bench.py --gpus N ...   (N > 1: one replica per GPU)
+    torchrun --nproc-per-node N bench.py --gpus N ...   (N > 1: one rank per GPU)
 
 Prints one JSON line.  `value` = uncompressed bytes of all ranks / (max over
 ranks of the device time of K steps); `e2e` = the same through the public API
 with pinned host buffers and the H2D/D2H copies inside the timed region.
-The path partitions by buffer, so N GPUs run N independent replicas (weak
-scaling, no collective on the data path).
+The path partitions by buffer: with N > 1 the batch's buffers are sharded
+across the ranks by bytes (strong scaling, no collective on the data path);
+`--replicas` gives every rank a whole batch instead (weak scaling).
 """
 from __future__ import annotations
 
@@ -573,7 +574,8 @@ def run_batch(args, rank, world, dev, pg):
                                        if shard else f"replicas x{world}"),
                        "step": "batched compress (device histograms, codebooks, encode) then batched "
                                "decompress, two captured CUDA graphs",
-                       "l2": "inputs (2.46 GB) larger than the 126 MB L2; no flush",
+                       "l2": (f"inputs ({total / 1e9:.2f} GB per GPU) larger than the 126 MB L2; no flush"
+                              if total > 126e6 else "inputs smaller than the 126 MB L2 (profiling size)"),
                        "compressed_bytes": C, "compressed_over_raw": round(C / total, 4),
                        "tuning": tuning},
             "encode_gbs": round(total / c_ms / 1e6, 1),
@@ -788,7 +790,7 @@ def main():
             "dtype": "u8", "data": "synthetic",
             "config": {"workload": desc, "bytes_per_gpu": n, "parallelism": f"replicas x{world}",
                        "step": "histogram -> codebook (host) -> encode -> decode",
-                       "l2": "input (1 GiB) larger than the 126 MB L2; no flush",
+                       "l2": f"input ({n / 2**20:.0f} MiB) larger than the 126 MB L2; no flush",
                        "compressed_bytes": C, "bits_per_byte": round(sizes.bits / n, 4)},
             "encode_gbs": round(n / (kern_ms["hist"] + kern_ms["encode"]) / 1e6, 1),
             "decode_gbs": round(n / kern_ms["decode"] / 1e6, 1),

@@ -86,7 +86,6 @@ __device__ inline void widen_tables(const DecTable& t, bool multi, DecTableW& w,
     const uint32_t groups = (*s_used + 7) / 8;
     for (uint32_t i = tid; i < groups; i += blockDim.x)
         reinterpret_cast<uint4*>(w.t2)[i] = reinterpret_cast<const uint4*>(t.t2)[i];
-    if (tid == 0) w.t2_groups = groups;
     __syncthreads();  // s1 and s_used are reused for the next buffer
 }
 

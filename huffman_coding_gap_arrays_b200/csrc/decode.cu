@@ -9,7 +9,8 @@
 //      shared memory (padded one word in eight so the threads' windows, 4
 //      words apart, fall in different banks) and every thread decodes its
 //      segments one after the other (interleaving two chains measured slower:
-//      the loop is issue-bound) through a shared-memory two-level table,
+//      the loop is issue-bound) through a two-level table (level 1 in shared
+//      memory, the rarely used level 2 read from global memory),
 //      parking each segment's symbols in its own shared row sized for the
 //      book's shortest code (a segment holds at most ceil(128 / shortest
 //      length) symbols);
@@ -56,9 +57,15 @@ struct DecCfg {
     static constexpr int kRow = ((kMaxSym + 4) / 4 | 1) * 4;
     static constexpr int kStageBytes = kSegs * kRow + 16;
     static constexpr int kCompactBytes = kSegs * kMaxSym + 64;
-    static constexpr size_t kSmem = (size_t)(kT1 + kT2 / 2 + kWordsPad + kGapStage) * 4 +
-                                    kStageBytes + kCompactBytes + kT1;  // + first-code lengths (u8)
-    static_assert(kT1 % 4 == 0 && (kT2 / 2) % 4 == 0 && kWordsPad % 4 == 0 && kGapStage % 4 == 0 &&
+    static constexpr int kL1Bytes = dec_multi(R, true) ? kT1 : 0;  // multi entries: first-code lengths
+    // the level-2 table stays in global memory (or the kernel parameter): codes longer
+    // than the 11-bit prefix are rare, and its 5 KiB buy a fourth CTA per SM for 8 and
+    // 16 stage rows (Zipf(1.2) 0.684 -> 0.592 ms, uniform bytes 0.570 -> 0.481 ms per
+    // 256 MiB); 11 rows stay at three, 32 rows at two
+    static constexpr int kMinBlocks = R == 32 ? 2 : 4;
+    static constexpr size_t kSmem = (size_t)(kT1 + kWordsPad + kGapStage) * 4 +
+                                    kStageBytes + kCompactBytes + kL1Bytes;
+    static_assert(kT1 % 4 == 0 && kWordsPad % 4 == 0 && kGapStage % 4 == 0 &&
                   kStageBytes % 16 == 0, "16-byte aligned areas");
 };
 
@@ -66,7 +73,7 @@ __device__ __forceinline__ uint32_t pidx(uint32_t w) { return w + (w >> 3); }
 
 // One codeword from the 32-bit window x at the current position: level-1
 // lookup, level 2 for the rare longer codes.  Returns the widened entry.
-__device__ __forceinline__ uint32_t lookup(const uint32_t* t1, const uint16_t* t2, uint32_t x) {
+__device__ __forceinline__ uint32_t lookup(const uint32_t* t1, const uint16_t* __restrict__ t2, uint32_t x) {
     uint32_t e = t1[x >> (32 - kDecPrefix)];
     if (e & 0x80000000u) {
         const uint32_t wd = (e >> 16) & 7u;
@@ -90,13 +97,12 @@ struct DecSlot {
 // (worth it for short-code books; for long codes the extra selects only cost);
 // with a complete book, up to three (multi entries, widen_multi).
 template <int R, bool COMPLETE, bool PAIRS>
-__global__ void __launch_bounds__(kDecThreads, 3)
+__global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
     decode_kernel(const __grid_constant__ DecArgs a, const __grid_constant__ DecTable tab) {
     using C = DecCfg<R>;
     extern __shared__ __align__(16) uint32_t smem[];
     uint32_t* t1 = smem;
-    uint16_t* t2 = reinterpret_cast<uint16_t*>(smem + C::kT1);
-    uint32_t* sw = smem + C::kT1 + C::kT2 / 2;
+    uint32_t* sw = smem + C::kT1;
     uint32_t* sg = sw + C::kWordsPad;                    // gap words: sg[j] = gaps[s0/8 - 1 + j]
     uint8_t* stage = reinterpret_cast<uint8_t*>(sg + C::kGapStage);
     uint8_t* compact = stage + C::kStageBytes;
@@ -119,7 +125,6 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                 t1[i] = PAIRS ? widen_pair(t.t1, i) : widen_entry(t.t1[i]);
             }
         }
-        for (int i = tid; i < C::kT2; i += kDecThreads) t2[i] = t.t2[i];
     };
     // batched path (always PAIRS): the buffer's tables come widened, copied in 16-byte groups
     auto copy_tables = [&](const DecTableW& t) {
@@ -129,9 +134,6 @@ __global__ void __launch_bounds__(kDecThreads, 3)
             const uint4* sl = reinterpret_cast<const uint4*>(t.l1);
             for (int i = tid; i < C::kT1 / 16; i += kDecThreads) reinterpret_cast<uint4*>(l1t)[i] = sl[i];
         }
-        const uint32_t g = t.t2_groups;
-        const uint4* s2 = reinterpret_cast<const uint4*>(t.t2);
-        for (uint32_t i = tid; i < g; i += kDecThreads) reinterpret_cast<uint4*>(t2)[i] = s2[i];
     };
     // thread 0: the tile `item` and its job into slot s
     auto fill_slot = [&](int s, uint64_t item) {
@@ -151,16 +153,19 @@ __global__ void __launch_bounds__(kDecThreads, 3)
     do {                                                                                      \
         const DecSlot& ps = slot[S];                                                          \
         const bool ok = ps.item < s_nitems;                                                   \
-        const uint64_t ps0 = ps.local * C::kSegs;                                             \
+        const uint64_t pw0 = ps.local * (4 * C::kSegs);  /* the tile's first word */          \
+        const uint64_t pg0 = ps.local * (C::kSegs / 8);  /* and first gap word */             \
+        const uint64_t wrem = ok && ps.job.words > pw0 ? ps.job.words - pw0 : 0;              \
+        const uint32_t wavail = wrem < (uint64_t)C::kWords ? (uint32_t)wrem : (uint32_t)C::kWords; \
+        const uint32_t* const wsrc = ps.job.bits + pw0;                                       \
         _Pragma("unroll") for (int j = 0; j < C::kWordsPer; ++j) {                            \
             const uint32_t i = tid + j * kDecThreads;                                         \
-            const uint64_t w = 4 * ps0 + i;                                                   \
-            pre[j] = (ok && i < (uint32_t)C::kWords && w < ps.job.words)                      \
-                         ? ld_stream_u32(ps.job.bits + w) : 0u;                               \
+            pre[j] = i < wavail ? ld_stream_u32(wsrc + i) : 0u;                               \
         }                                                                                     \
-        const int64_t g = (int64_t)(ps0 / 8) - 1 + (int64_t)tid;                              \
-        pre_gap = (ok && tid < (uint32_t)C::kGapStage && g >= 0 &&                            \
-                   (uint64_t)g < ps.job.gap_words) ? __ldg(ps.job.gaps + g) : 0u;             \
+        /* sg[j] = gaps[pg0 - 1 + j]: j = 0 exists unless the tile is its job's first */     \
+        const uint64_t grem = ok && ps.job.gap_words + 1 > pg0 ? ps.job.gap_words + 1 - pg0 : 0; \
+        const uint32_t gavail = grem < (uint64_t)C::kGapStage ? (uint32_t)grem : (uint32_t)C::kGapStage; \
+        pre_gap = (tid < gavail && (tid > 0 || pg0 > 0)) ? __ldg(ps.job.gaps + pg0 - 1 + tid) : 0u; \
     } while (0)
 #define HGAP_COMMIT()                                                                         \
     do {                                                                                      \
@@ -198,12 +203,19 @@ __global__ void __launch_bounds__(kDecThreads, 3)
         uint32_t claim = 0;
         if (tid == 0 && have) claim = atomicAdd(a.counter, 1u);  // its latency hides behind the decode
         const uint64_t s0 = T.local * C::kSegs;  // first segment of the tile within its job
-        const uint64_t segments = T.job.segments;
-        const uint64_t stream_bits = T.job.words * 32;
-        auto gap_of = [&](uint64_t k) -> uint32_t {  // k in [s0 - 1, s0 + 512)
-            const uint32_t j = (uint32_t)((k >> 3) - (s0 >> 3) + 1);
-            return (sg[j] >> (4 * (uint32_t)(k & 7))) & 0xfu;
-        };
+        const uint16_t* const t2 = a.jobs ? a.tables[T.job_id].t2 : tab.t2;  // level 2, not staged
+        // tile-local, 32-bit from here on: segments [0, nseg) of the tile; the stream's last
+        // segment (if in this tile) ends at bit end_last instead of at its 128-bit boundary
+        const uint64_t seg_rem = have ? T.job.segments - s0 : 0;
+        const uint32_t nseg = seg_rem < (uint64_t)C::kSegs ? (uint32_t)seg_rem : (uint32_t)C::kSegs;
+        const bool last_tile = seg_rem <= (uint64_t)C::kSegs;
+        // (every entry point checks segments == ceil(words / 4); the clamp keeps any
+        // other job inside its staged words)
+        const uint64_t bits_rem = last_tile && have ? T.job.words * 32 - 128 * s0 : 0;
+        const uint32_t end_last = bits_rem < 128ull * nseg ? (uint32_t)bits_rem : 128 * nseg;
+        const uint32_t first_gap = s0 ? ~0u : 0u;  // the job's first segment starts at bit 0
+        // gap entry of tile segment u - 8 (u >= 7: u = 7 is the segment before the tile)
+        auto gap_at = [&](uint32_t u) -> uint32_t { return (sg[u >> 3] >> (4 * (u & 7))) & 0xfu; };
 
         // ---- 1. decode segments tid (and tid + 256), one after the other -------
         uint32_t n[2] = {0, 0};
@@ -211,13 +223,11 @@ __global__ void __launch_bounds__(kDecThreads, 3)
 #pragma unroll
             for (int k = 0; k < C::kPer; ++k) {
                 const uint32_t col = tid + k * kDecThreads;
-                const uint64_t s = s0 + col;
                 uint32_t cnt = 0;
-                if (s < segments) {
-                    const bool last = s + 1 == segments;
-                    uint32_t pos = 128 * col + (s ? gap_of(s - 1) : 0u);
-                    uint32_t end = 128 * col + 128;
-                    if (last && stream_bits - 128 * s0 < end) end = (uint32_t)(stream_bits - 128 * s0);
+                if (col < nseg) {
+                    const bool last = last_tile && col + 1 == nseg;
+                    uint32_t pos = 128 * col + (gap_at(col + 7) & (col ? ~0u : first_gap));
+                    const uint32_t end = last ? end_last : 128 * col + 128;
                     bool bad = false;
                     uint8_t* const row = stage + col * C::kRow;
                     uint8_t* out = row;
@@ -314,7 +324,7 @@ __global__ void __launch_bounds__(kDecThreads, 3)
                         }
                     }
                     cnt = (uint32_t)(out - row);
-                    if (!last && !bad && pos != 128 * col + 128 + gap_of(s)) bad = true;
+                    if (!last && !bad && pos != 128 * col + 128 + gap_at(col + 8)) bad = true;
                     if (bad) atomicOr(a.status, kDevCorrupt);
                 }
                 n[k] = cnt;

@@ -156,17 +156,16 @@ struct DecTable {
 constexpr int kDecMultiMinRows = 32;
 HGAP_HD constexpr bool dec_multi(int rows, bool complete) { return complete && rows >= kDecMultiMinRows; }
 
-// The decode kernel's shared-memory tables in their widened form (u32 level-1
-// entries: pair form, or multi form for a complete book, with the length of
-// the first code per prefix), built once per buffer on the batched path so
-// that a CTA moving to another buffer's tile copies them with 16-byte loads
-// instead of re-deriving every entry.  Only the level-2 groups in use travel.
+// The decode kernel's level-1 tables in their widened form (u32 entries: pair
+// form, or multi form for a complete book, with the length of the first code
+// per prefix), built once per buffer on the batched path so that a CTA moving
+// to another buffer's tile copies them into shared memory with 16-byte loads
+// instead of re-deriving every entry.  The level-2 table (its groups in use)
+// is read from here directly.
 struct DecTableW {
     uint32_t t1[1 << kDecPrefix];
     uint8_t l1[1 << kDecPrefix];
     uint16_t t2[kDecT2Cap];
-    uint32_t t2_groups;  // 16-byte groups of t2 in use
-    uint32_t pad[3];
 };
 static_assert(sizeof(DecTableW) % 16 == 0, "16-byte copies");
 

@@ -24,6 +24,7 @@ comparison -- requests run one by one through the plain single-buffer path.
 from __future__ import annotations
 
 import ctypes as C
+import gc
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -90,7 +91,7 @@ class Server:
     def __init__(self, policy: str = "batched", tuner=None, config: LaunchConfig | None = None,
                  hbm_budget: float = 40e9, max_batch: int = 64, max_inflight: int = 3,
                  traffic_features=(5.0, 12.0, 0.05), device="cuda", keep_results: bool = False,
-                 reserve_bytes: int = 4 << 30):
+                 reserve_bytes: int = 8 << 30):
         if policy not in ("batched", "plain"):
             raise ValueError("policy is 'batched' or 'plain'")
         self.policy = policy
@@ -106,12 +107,10 @@ class Server:
         self.free_streams = list(self.streams)  # a new batch only goes to a stream with nothing queued
         if reserve_bytes and self.policy == "batched":
             # one large cached block up front: per-batch allocations of varying size are
-            # then carved from it instead of each new size reaching the driver mid-run
-            for s_ in self.streams:
-                with torch.cuda.stream(s_):
-                    blk = torch.empty(int(reserve_bytes) // len(self.streams), dtype=torch.uint8,
-                                      device=self.device)
-                    del blk
+            # then carved from it instead of each new size reaching the driver mid-run.
+            # Every batch allocates on the current stream (one pool; see _launch).
+            blk = torch.empty(int(reserve_bytes), dtype=torch.uint8, device=self.device)
+            del blk
         self.held = 0
         self.peak_held = 0
         self.batches = 0
@@ -146,28 +145,34 @@ class Server:
         cfg = self._config_for(reqs)
         comp = [r for r in reqs if r.kind == "compress"]
         dec = [r for r in reqs if r.kind == "decompress"]
+        # Allocations and uploads on the current stream: the caching allocator keeps one
+        # pool per stream, and a batch's blocks taken from one shared pool (freed only
+        # after the batch's event has fired) never send a new size to the driver mid-run
+        # just because the batch landed on another stream than the last one of that size.
+        plan = ent = None
+        if comp:
+            plan = BatchCodec([r.data.numel() for r in comp], cfg, device=self.device)
+            plan.bind([r.data for r in comp])
+            ent = torch.empty(plan.entries.numel(), dtype=torch.uint8, pin_memory=True)
+        dprep = self._decompress_prepare(dec) if dec else None
         s.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(s):
             if comp:
-                plan = BatchCodec([r.data.numel() for r in comp], cfg, device=self.device)
-                plan.bind([r.data for r in comp])
                 plan.compress(stream=s)
-                ent = torch.empty(plan.entries.numel(), dtype=torch.uint8, pin_memory=True)
                 ent.copy_(plan.entries, non_blocking=True)
                 b.plan, b.entries_host = plan, ent
                 b.keep.append((comp, plan, ent))
             if dec:
-                outs = [torch.empty(max(r.nbytes, 1), dtype=torch.uint8, device=self.device) for r in dec]
-                self._decompress(dec, outs, cfg, s, b)
-                for r, o in zip(dec, outs):
-                    r.result = o[:r.nbytes]
+                self._decompress_launch(dec, dprep, cfg, s, b)
         b.event.record(s)
         return b
 
-    def _decompress(self, reqs, outs, cfg, s, b) -> None:
+    def _decompress_prepare(self, reqs):
         """One batched decompress over streams that live anywhere in device
-        memory: each entry's offsets are rebased on the lowest address."""
+        memory: each entry's offsets are rebased on the lowest address.  The
+        outputs, tables and workspace, allocated and uploaded on the current stream."""
         count = len(reqs)
+        outs = [torch.empty(max(r.nbytes, 1), dtype=torch.uint8, device=self.device) for r in reqs]
         base_b = min(r.stream.bits.data_ptr() for r in reqs) & ~15
         base_g = min(r.stream.gaps.data_ptr() for r in reqs) & ~3
         arr = (BatchEntry * count)()
@@ -180,10 +185,16 @@ class Server:
         sizes = np.array([r.nbytes for r in reqs], np.uint64)
         nbytes = lib().hgap_batch_decompress_workspace_bytes(count, sizes.ctypes.data_as(C.POINTER(C.c_uint64)))
         ws = torch.empty((nbytes + 7) // 8, dtype=torch.int64, device=self.device)
+        return outs, base_b, base_g, d_ent, d_out, ws
+
+    def _decompress_launch(self, reqs, prep, cfg, s, b) -> None:
+        outs, base_b, base_g, d_ent, d_out, ws = prep
         c = cfg.cstruct()
-        check(lib().hgap_batch_decompress(count, d_ent.data_ptr(), base_b, base_g, d_out.data_ptr(),
+        check(lib().hgap_batch_decompress(len(reqs), d_ent.data_ptr(), base_b, base_g, d_out.data_ptr(),
                                           ws.data_ptr(), ws.numel() * 8, C.byref(c), _stream(s)),
               "hgap_batch_decompress")
+        for r, o in zip(reqs, outs):
+            r.result = o[:r.nbytes]
         b.keep.append((reqs, d_ent, d_out, ws, outs))
         b.dec_ws = ws
 
@@ -216,13 +227,23 @@ class Server:
         """Serves `requests` (sorted by arrival) in real time; returns the
         latency and throughput statistics."""
         reqs = sorted(requests, key=lambda r: r.arrival)
-        if self.policy == "plain":
-            return self._run_plain(reqs)
-        if self.tuner is not None and hasattr(self.tuner, "precompute"):
+        if self.policy != "plain" and self.tuner is not None and hasattr(self.tuner, "precompute"):
             # every batch size the run can form, decided before the clock starts
             sizes = [r.nbytes for r in reqs]
             self.tuner.precompute(self.traffic, np.log2(max(1, min(sizes))),
                                   np.log2(max(1, sum(sorted(sizes)[-self.max_batch:]))))
+        # the cyclic garbage collector stays off while the clock runs: a full pass over
+        # the run's objects stalled a launch for ~100 ms and every request queued behind it
+        gc_on = gc.isenabled()
+        gc.collect()
+        gc.disable()
+        try:
+            return self._run_plain(reqs) if self.policy == "plain" else self._loop(reqs)
+        finally:
+            if gc_on:
+                gc.enable()
+
+    def _loop(self, reqs) -> dict:
         pending = deque(reqs)
         queue = deque()
         inflight = []
