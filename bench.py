@@ -475,6 +475,12 @@ def run_batch(args, rank, world, dev, pg):
     plain = None
     kp = min(args.plain_buffers, len(sizes))
     if kp:
+        # one untimed pass first: the allocator's pools see every size once, as the batched
+        # path's workspaces were allocated before its clock started
+        warm = [H.compress(x) for x in ins[:kp]]
+        del warm
+        warm = [H.decompress(H.compress(x)) for x in ins[:min(kp, 64)]]
+        del warm
         torch.cuda.synchronize()
         a = time.perf_counter()
         comp = [H.compress(x) for x in ins[:kp]]
@@ -490,7 +496,7 @@ def run_batch(args, rank, world, dev, pg):
                  "decompress_gbs": round(sub / (c_ - b_) / 1e9, 3),
                  "roundtrip_gbs": round(sub / (c_ - a) / 1e9, 3),
                  "how": "codec.compress / codec.decompress per buffer (histogram -> host codebook -> "
-                        "encode; decode), wall clock with device syncs"}
+                        "encode; decode), wall clock with device syncs, after one untimed pass"}
         del comp, dec_out
 
     # ---- end to end through the public API, host buffers ---------------------

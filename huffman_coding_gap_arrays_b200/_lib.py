@@ -23,7 +23,7 @@ STATUS_NAMES = {
 EXPORTS = [
     "hgap_status_string", "hgap_histogram", "hgap_codebook_build", "hgap_codebook_from_symbols",
     "hgap_sizes_from_bits", "hgap_encoded_bits", "hgap_encode_workspace_bytes", "hgap_encode",
-    "hgap_encode_histogram", "hgap_encode_prepared",
+    "hgap_encode_histogram", "hgap_encode_prepared", "hgap_encode_part_prepared",
     "hgap_decode_workspace_bytes", "hgap_decode", "hgap_workspace_status", "hgap_container_bytes",
     "hgap_container_write", "hgap_container_parse", "histgram", "hgap_ref_encode",
     "hgap_ref_decoder_l1_l2", "hgap_decode_noalloc", "hgap_codebook_build_device",
@@ -102,6 +102,8 @@ def lib() -> C.CDLL:
     L.hgap_encode.argtypes = [vp, u64, C.POINTER(CCodebook), vp, u64, vp, u64, vp, C.c_size_t, vp]
     L.hgap_encode_prepared.argtypes = L.hgap_encode.argtypes
     L.hgap_encode_histogram.argtypes = [vp, u64, vp, vp, C.c_size_t, vp]
+    L.hgap_encode_part_prepared.argtypes = [vp, u64, C.POINTER(CCodebook), u64, u64, vp, u64, vp, u64, vp,
+                                            C.c_size_t, vp]
     L.hgap_decode_workspace_bytes.argtypes = [u64]
     L.hgap_decode_workspace_bytes.restype = C.c_size_t
     L.hgap_decode.argtypes = [vp, u64, vp, u64, C.POINTER(CCodebook), vp, u64, vp, C.c_size_t, vp]
@@ -144,7 +146,8 @@ def lib() -> C.CDLL:
                  "hgap_mlp_loss_grad", "hgap_mlp_adam"):
         getattr(L, name).restype = C.c_int
     for name in ("hgap_histogram", "hgap_codebook_build", "hgap_codebook_from_symbols",
-                 "hgap_encode", "hgap_encode_histogram", "hgap_encode_prepared", "hgap_decode", "hgap_workspace_status", "hgap_container_write",
+                 "hgap_encode", "hgap_encode_histogram", "hgap_encode_prepared", "hgap_encode_part_prepared",
+                 "hgap_decode", "hgap_workspace_status", "hgap_container_write",
                  "hgap_container_parse", "hgap_ref_encode", "hgap_ref_decoder_l1_l2",
                  "hgap_decode_noalloc"):
         getattr(L, name).restype = C.c_int

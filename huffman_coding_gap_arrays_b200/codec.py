@@ -188,6 +188,35 @@ class Encoder:
             self.check(stream)
         return bits[:sizes.words], gaps[:sizes.gap_words]
 
+    def encode_part(self, x: torch.Tensor, book: Codebook, bit0: int, part_bits: int, stream=None,
+                    check_status: bool = True):
+        """One part of a stream split across devices (hgap_encode_part_prepared),
+        after ``histogram(x)`` on this encoder: x's codes placed from stream bit
+        ``bit0``.  Returns (first stream word, its words, first gap word, its
+        gap words); the stream is the OR of all parts' words at those places
+        (``parallel.stitch_parts``)."""
+        _require_cuda(x, "x")
+        n = x.numel() * x.element_size()
+        if n > self.capacity:
+            raise ValueError(f"input of {n} bytes exceeds encoder capacity {self.capacity}")
+        bit0, part_bits = int(bit0), int(part_bits)
+        end = bit0 + part_bits
+        w_first, g_first = bit0 >> 5, bit0 >> 10
+        w_base = w_first & ~3                        # the window starts on a 16-byte boundary
+        w_end, g_end = (end + 31) // 32, ((end + 127) // 128 + 7) // 8
+        bits = torch.empty(max(w_end - w_base, 1), dtype=torch.int32, device=x.device)
+        gaps = torch.empty(max(g_end - g_first, 1), dtype=torch.int32, device=x.device)
+        ws = self.workspace
+        check(lib().hgap_encode_part_prepared(x.data_ptr(), n, C.byref(book.cstruct), bit0, part_bits,
+                                              bits.data_ptr(), w_base, gaps.data_ptr(), g_first,
+                                              ws.data_ptr(), ws.numel() * 8, _stream(stream)),
+              "hgap_encode_part_prepared")
+        if check_status and n:
+            self.check(stream)
+        if n == 0:
+            return w_first, bits[:0], g_first, gaps[:0]
+        return w_first, bits[w_first - w_base:w_end - w_base], g_first, gaps[:g_end - g_first]
+
     def check(self, stream=None) -> None:
         check(lib().hgap_workspace_status(self.workspace.data_ptr(), _stream(stream)), "encode (device)")
 

@@ -142,6 +142,36 @@ hgap_status hgap_encode_prepared(const void* d_in, uint64_t n, const hgap_codebo
     return cuda_status(hgap::launch_encode(a, t, 0, stream));
 }
 
+hgap_status hgap_encode_part_prepared(const void* d_in, uint64_t n, const hgap_codebook* cb, uint64_t bit0,
+                                      uint64_t part_bits, uint32_t* d_bits, uint64_t bits_word0,
+                                      uint32_t* d_gaps, uint64_t gaps_word0, void* d_workspace,
+                                      size_t workspace_bytes, hgap_stream_t stream) {
+    if (!cb) return HGAP_ERR_INVALID_ARG;
+    if (n == 0) return part_bits == 0 ? HGAP_OK : HGAP_ERR_SIZE;
+    if ((bits_word0 & 3) || bits_word0 > (bit0 >> 5) || gaps_word0 > (bit0 >> 10)) return HGAP_ERR_INVALID_ARG;
+    const uint64_t end = bit0 + part_bits;
+    if (end < bit0) return HGAP_ERR_SIZE;
+    hgap::EncArgs a;
+    hgap::HistStArgs h;
+    hgap_status s = encode_layout(d_in, n, d_workspace, workspace_bytes, &a, &h);
+    // the stream's word and segment counts through the end of this part
+    if (s == HGAP_OK) s = encode_outputs(cb, d_bits, (end + 31) / 32, d_gaps, (end + 127) / 128, &a);
+    if (s != HGAP_OK) return s;
+    // the windows hold stream words [bits_word0, ..) and gap words [gaps_word0, ..): the job
+    // addresses stream word w at bits + w, never below bits_word0 (w >= bit0 / 32), and
+    // bits_word0 % 4 == 0 keeps the 16-byte alignment of the window's vector stores
+    hgap::EncJob& J = a.single;
+    J.bits = reinterpret_cast<uint32_t*>(reinterpret_cast<uintptr_t>(d_bits) - 4 * bits_word0);
+    J.gaps = reinterpret_cast<uint32_t*>(reinterpret_cast<uintptr_t>(d_gaps) - 4 * gaps_word0);
+    J.bit0 = bit0;
+    hgap::EncTable t;
+    hgap::make_enc_table(*cb, &t);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    s = encode_clear(a, false, st);
+    if (s != HGAP_OK) return s;
+    return cuda_status(hgap::launch_encode(a, t, 0, stream));
+}
+
 hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
                         uint64_t words, uint32_t* d_gaps, uint64_t segments, void* d_workspace,
                         size_t workspace_bytes, hgap_stream_t stream) {

@@ -361,51 +361,45 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
         __syncthreads();  // (3) prev's output offset known
 
         // ---- 3. write out prev: 16-byte output chunk q takes compact bytes
-        //         [16q - vstart, 16q - vstart + 16), i.e. parts of two aligned groups
+        //         [16q - base, 16q - base + 16), i.e. parts of two aligned groups
         if (prev_s >= 0) {
             const DecSlot& Pv = slot[prev_s];
             const uint64_t O = s_O;
             const uint32_t Cp = prev_ct;
             const uint64_t nout = Pv.job.n;
-            uint8_t* const out_al = Pv.job.out_aligned;
             if (tid == 0 && Pv.local + 1 == Pv.job.ntiles && O + Cp < nout) atomicOr(a.status, kDevSize);
             if (O < nout) {
                 const uint64_t vstart = Pv.job.out_lo + O;
-                const uint64_t vend = Pv.job.out_lo + (O + Cp < nout ? O + Cp : nout);
                 const uint32_t base = (uint32_t)(vstart & 15);  // compact byte 0 sits at chunk offset base
-                const uint64_t q0 = vstart >> 4, q1 = (vend + 15) >> 4;
-                const uint32_t nq = (uint32_t)(q1 - q0);
-                for (uint32_t i0q = warp * 32; i0q < nq; i0q += kDecThreads) {
-                    const uint32_t lq = i0q + lane;  // chunk index within the tile
-                    // aligned compact group lq covers chunk lq's bytes [base, 16) and chunk lq+1's [0, base)
-                    uint4 g = make_uint4(0, 0, 0, 0);
-                    if (lq < nq) g = *reinterpret_cast<const uint4*>(compact + 16 * lq);
-                    uint4 p;  // group lq - 1
-                    p.x = __shfl_up_sync(kFull, g.x, 1);
-                    p.y = __shfl_up_sync(kFull, g.y, 1);
-                    p.z = __shfl_up_sync(kFull, g.z, 1);
-                    p.w = __shfl_up_sync(kFull, g.w, 1);
-                    if (lane == 0 && lq > 0) p = *reinterpret_cast<const uint4*>(compact + 16 * (lq - 1));
-                    if (lq >= nq) continue;
+                // tile-local byte positions from here on: [base, vend) of chunks 0..nq-1
+                const uint32_t vend = base + (O + Cp < nout ? Cp : (uint32_t)(nout - O));
+                const uint32_t nq = (vend + 15) >> 4;
+                uint8_t* const out0 = Pv.job.out_aligned + (vstart & ~15ull);  // 16-byte aligned
+                const uint32_t sh = 8 * (base & 3), sel = base >> 2;
+                auto comb = [sh](uint32_t lo, uint32_t hi) { return sh ? __funnelshift_r(lo, hi, 32 - sh) : hi; };
+                for (uint32_t lq = tid; lq < nq; lq += kDecThreads) {
+                    // aligned group lq holds chunk lq's bytes [base, 16) and chunk lq+1's
+                    // [0, base); group lq - 1 (for lq = 0 the stage's slack: bytes below
+                    // base, never stored) the rest
+                    const uint4 g = *reinterpret_cast<const uint4*>(compact + 16 * lq);
+                    const uint4 p = *reinterpret_cast<const uint4*>(compact + 16 * lq - 16);
                     // output byte b = byte 16 - base + b of the 32-byte pair (p, g): output word i
                     // joins words k and k+1 of (p.x..p.w, g.x..g.w), k = 3 - base/4 + i
-                    const uint32_t sh = 8 * (base & 3);
-                    auto comb = [sh](uint32_t lo, uint32_t hi) { return sh ? __funnelshift_r(lo, hi, 32 - sh) : hi; };
                     uint32_t o[4];
-                    switch (base >> 2) {  // uniform over the tile
+                    switch (sel) {  // uniform over the tile
                         case 0: o[0] = comb(p.w, g.x); o[1] = comb(g.x, g.y); o[2] = comb(g.y, g.z); o[3] = comb(g.z, g.w); break;
                         case 1: o[0] = comb(p.z, p.w); o[1] = comb(p.w, g.x); o[2] = comb(g.x, g.y); o[3] = comb(g.y, g.z); break;
                         case 2: o[0] = comb(p.y, p.z); o[1] = comb(p.z, p.w); o[2] = comb(p.w, g.x); o[3] = comb(g.x, g.y); break;
                         default: o[0] = comb(p.x, p.y); o[1] = comb(p.y, p.z); o[2] = comb(p.z, p.w); o[3] = comb(p.w, g.x); break;
                     }
-                    const uint64_t c0 = (q0 + lq) << 4;
-                    if (c0 >= vstart && c0 + 16 <= vend) {
-                        *reinterpret_cast<uint4*>(out_al + c0) = make_uint4(o[0], o[1], o[2], o[3]);
-                    } else {
+                    const uint32_t c0 = 16 * lq;
+                    if (c0 >= base && c0 + 16 <= vend) {
+                        *reinterpret_cast<uint4*>(out0 + c0) = make_uint4(o[0], o[1], o[2], o[3]);
+                    } else {  // the two ragged chunks
 #pragma unroll
                         for (uint32_t b = 0; b < 16; ++b) {
-                            const uint64_t vb = c0 + b;
-                            if (vb >= vstart && vb < vend) out_al[vb] = (uint8_t)(o[b >> 2] >> (8 * (b & 3)));
+                            const uint32_t vb = c0 + b;
+                            if (vb >= base && vb < vend) out0[vb] = (uint8_t)(o[b >> 2] >> (8 * (b & 3)));
                         }
                     }
                 }
@@ -423,7 +417,9 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
                 const uint32_t d = excl[k], m = n[k];
                 uint32_t h = (4u - (d & 3u)) & 3u;
                 if (h > m) h = m;
-                for (uint32_t j = 0; j < h; ++j) compact[d + j] = src[j];
+                if (h > 0) compact[d] = src[0];
+                if (h > 1) compact[d + 1] = src[1];
+                if (h > 2) compact[d + 2] = src[2];
                 const uint32_t nwords = (m - h) >> 2;
                 const uint32_t* sw32 = reinterpret_cast<const uint32_t*>(src);
                 uint32_t* dw = reinterpret_cast<uint32_t*>(compact + d + h);
@@ -434,7 +430,10 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
                     dw[j] = __funnelshift_r(lo, hi, sh);
                     lo = hi;
                 }
-                for (uint32_t j = h + 4 * nwords; j < m; ++j) compact[d + j] = src[j];
+                const uint32_t t = h + 4 * nwords, tl = m - t;  // 0..3 last bytes
+                if (tl > 0) compact[d + t] = src[t];
+                if (tl > 1) compact[d + t + 1] = src[t + 1];
+                if (tl > 2) compact[d + t + 2] = src[t + 2];
             }
         }
         if (have_next) {  // sw/sg and the tables are no longer read for this tile

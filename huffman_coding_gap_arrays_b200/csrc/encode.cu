@@ -216,7 +216,8 @@ __global__ void __launch_bounds__(kEncThreads, 2)
 
         // ---- warp 0: G of the current region, bits before G ---------------------
         if (warp == 0) {
-            const uint64_t G = lookback_resolve<4>(a.st_rec, item, sh.agg[cur_slot], st == 0, a.status, lane);
+            const uint64_t G =
+                J.bit0 + lookback_resolve<4>(a.st_rec, item, sh.agg[cur_slot], st == 0, a.status, lane);
             uint32_t head = 0, gcarry = 0;
             const uint32_t r = (uint32_t)(G & 31);
             const uint32_t nibs = (uint32_t)((G >> 7) & 7);

@@ -95,6 +95,9 @@ struct EncJob {
     uint64_t nst;               // its regions
     uint32_t st_bytes;          // region size in input bytes (a multiple of kEncChunkBytes)
     uint32_t bits_aligned16;    // bits is 16-byte aligned: vector stores allowed
+    uint64_t bit0;              // stream bit of the job's first code: 0, unless the job is one
+                                // part of a stream split across devices (bits / gaps then
+                                // address stream word / gap word 0 of a window)
 };
 
 struct EncArgs {

@@ -136,6 +136,27 @@ hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, u
                         uint64_t words, uint32_t* d_gaps, uint64_t segments, void* d_workspace,
                         size_t workspace_bytes, hgap_stream_t stream);
 
+/* One part of a stream split across devices (no counterpart in the reference):
+ * each device encodes a contiguous byte range of one buffer.  The parts share
+ * one codebook, built from the sum of the parts' histograms, and part p starts
+ * at stream bit bit0 = the sum of the earlier parts' bit counts
+ * (hgap_encoded_bits of each part's histogram: an exclusive scan of one 8-byte
+ * value per device).  Call after hgap_encode_histogram on this part (same
+ * input, same workspace).
+ * d_bits is a window holding stream words [bits_word0, ceil((bit0 +
+ * part_bits) / 32)), bits_word0 a multiple of 4 and <= bit0 / 32; d_gaps a
+ * window holding gap words [gaps_word0, ceil(ceil((bit0 + part_bits) / 128) /
+ * 8)), gaps_word0 <= bit0 / 1024.  Window words before bit0 / 32 (gap words
+ * before bit0 / 1024) are not written.  The word holding bit0 and the one
+ * holding the part's last bit carry only this part's bits (zeros elsewhere),
+ * and the first and last gap words only this part's entries -- entry k
+ * belongs to the part with bit0 < 128(k+1) <= bit0 + part_bits -- so the
+ * whole stream is the OR of all parts' windows, word by word. */
+hgap_status hgap_encode_part_prepared(const void* d_in, uint64_t n, const hgap_codebook* cb, uint64_t bit0,
+                                      uint64_t part_bits, uint32_t* d_bits, uint64_t bits_word0,
+                                      uint32_t* d_gaps, uint64_t gaps_word0, void* d_workspace,
+                                      size_t workspace_bytes, hgap_stream_t stream);
+
 /* --------------------------------------------------------------------- decode
  * Replaces void decoder_l1_l2(unsigned* input, int inputfilesize,
  * unsigned* output, int outputfilesize, int gap_elements, void* dectable,
