@@ -87,13 +87,14 @@ def peak_hbm():
 def traffic_ratios():
     """DRAM bytes per uncompressed byte per kernel, from the committed ncu summary."""
     out = {}
-    path = os.path.join(ROOT, "profiles", "dram_traffic_mixed_1g.txt")
-    if not os.path.exists(path):
-        return out
-    for line in open(path):
-        parts = line.split()
-        if len(parts) >= 3 and parts[0] == "traffic_per_input_byte":
-            out[parts[1]] = float(parts[2])
+    for name in ("dram_traffic_mixed_1g.txt", "dram_traffic_batch1024.txt"):
+        path = os.path.join(ROOT, "profiles", name)
+        if not os.path.exists(path):
+            continue
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 3 and parts[0] == "traffic_per_input_byte":
+                out[parts[1]] = float(parts[2])
     return out
 
 
