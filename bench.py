@@ -595,7 +595,7 @@ def run_batch(args, rank, world, dev, pg):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": 16 * args.steps,
+            "gpu_launches": (B.COMPRESS_KERNELS + B.DECOMPRESS_KERNELS) * args.steps,
             "clocks": clock_info,
         }
         print(json.dumps(line), flush=True)

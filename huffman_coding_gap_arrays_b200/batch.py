@@ -23,6 +23,11 @@ from ._lib import BatchConfig, BatchEntry, CCodebook, check, lib
 from .codec import Codebook, Compressed, StreamSizes, _stream
 
 ENTRY_BYTES = C.sizeof(BatchEntry)
+# Kernels one batched call launches (csrc/batch.cu): compress = benc_setup, hist_st, book,
+# benc_place, encode; decompress = bdec_book, bdec_widen, bdec_setup, bdec_map and one decoder
+# per class (8).
+COMPRESS_KERNELS = 5
+DECOMPRESS_KERNELS = 12
 
 
 @dataclass
