@@ -31,7 +31,7 @@ from .tuner import DEC_CTAS, Autotuner, compress_space
 
 SHAPES = [(32, 8), (32,), (32, 32), (32,), (2, 32), (2,)]
 # CTAs per SM that "0" (the occupancy maximum) means for each grid on B200
-MAX_CTAS = {"hist": 4, "enc": 2, "dec": 3}
+MAX_CTAS = {"hist": 4, "enc": 2, "dec": 4}
 
 
 def config_vector(cfg: LaunchConfig) -> np.ndarray:

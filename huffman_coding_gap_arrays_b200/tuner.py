@@ -28,7 +28,7 @@ from .batch import BatchCodec, LaunchConfig
 REGIONS = (1, 2, 4, 8, 16, 32)
 HIST_CTAS = (2, 4)
 ENC_CTAS = (1, 2)
-DEC_CTAS = (1, 2, 3)
+DEC_CTAS = (1, 2, 3, 4)  # decoder CTAs per SM; each stage size is clamped to what fits (4, 3 or 2)
 
 
 def compress_space():
