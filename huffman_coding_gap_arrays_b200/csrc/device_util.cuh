@@ -73,7 +73,8 @@ __device__ __forceinline__ uint64_t wait_nonzero(const uint64_t* p, uint32_t* st
 // ------------------------------------------- bulk copies into shared memory --
 // One-dimensional bulk copy (the TMA engine, no tensor map) from global to
 // this CTA's shared memory, completing on an mbarrier with a byte count.
-// Both addresses 16-byte aligned, size a multiple of 16.  Never multicast.
+// Both addresses 16-byte aligned, size a multiple of 16; the copy lands in this
+// CTA alone.
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
