@@ -71,6 +71,8 @@ def parse():
     p.add_argument("--serve-gbs", type=float, default=20.0, help="offered load of the serving run")
     p.add_argument("--cpu-sample-mib", type=int, default=256)
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--e2e-groups", type=int, default=32, help="batched e2e: groups of consecutive buffers")
+    p.add_argument("--e2e-streams", type=int, default=4, help="batched e2e: streams the groups take in turn")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()
 
@@ -502,11 +504,13 @@ def run_batch(args, rank, world, dev, pg):
 
     # ---- end to end through the public API, host buffers ---------------------
     # The batch in groups of consecutive buffers, each with its own plan and graphs, spread
-    # over three streams: one group's uploads run while another's downloads and kernels do
+    # over a few streams: one group's uploads run while another's downloads and kernels do
     # (PCIe is full duplex), where a single plan would copy in, compute and copy out in turn.
+    # Measured per step (groups x streams): 1 plan 150 ms, 4x2 104 ms, 8x3 95 ms, 16x4 90 ms,
+    # 32x4 89 ms -- 3.8 GB each way, ~43 GB/s per direction at once: the link, not the GPU.
     e2e = None
     if not args.no_e2e:
-        ngroups = max(1, min(8, len(sizes)))
+        ngroups = max(1, min(args.e2e_groups, len(sizes)))
         offs = [0]
         for n in sizes:
             offs.append(offs[-1] + n)
@@ -537,7 +541,7 @@ def run_batch(args, rank, world, dev, pg):
         in_host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
         in_host.copy_(flat)
         out_host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
-        streams = [torch.cuda.Stream(device=dev) for _ in range(3)]
+        streams = [torch.cuda.Stream(device=dev) for _ in range(max(1, args.e2e_streams))]
 
         def e2e_step():
             cur = torch.cuda.current_stream(dev)
@@ -585,7 +589,7 @@ def run_batch(args, rank, world, dev, pg):
         e2e = {"value": round(job_bytes * e2e_steps / e_ms / 1e6, 3), "unit": "GB/s",
                "h2d_bytes_per_step": total + cont, "d2h_bytes_per_step": cont + total,
                "ms_per_step": round(e_ms / e2e_steps, 3),
-               "how": f"{len(groups)} groups of consecutive buffers on 3 streams: upload, compress, "
+               "how": f"{len(groups)} groups of consecutive buffers on {len(streams)} streams: upload, compress, "
                       "container down and up again, decompress, download; each group's copies and "
                       "kernels in order, groups overlapping"}
         del groups
