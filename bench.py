@@ -352,6 +352,102 @@ def run_serving(args, pool, learned, fixed_cfg, dev):
     return out
 
 
+def run_e2e_batch(args, sizes, flat, flat_out, ins, outs, cfg, total, job_bytes, dev, pg, stream):
+    """The batched round trip through host memory (see `e2e` in the module
+    docstring); everything it allocates is released when it returns."""
+    import numpy as np
+    import torch
+    from huffman_coding_gap_arrays_b200 import batch as B
+    # The batch in groups of consecutive buffers, each with its own plan and graphs, spread
+    # over a few streams: one group's uploads run while another's downloads and kernels do
+    # (PCIe is full duplex), where a single plan would copy in, compute and copy out in turn.
+    # Measured per step (groups x streams): 1 plan 150 ms, 4x2 104 ms, 8x3 95 ms, 16x4 90 ms,
+    # 32x4 89 ms -- 3.8 GB each way, ~43 GB/s per direction at once: the link, not the GPU.
+    ngroups = max(1, min(args.e2e_groups, len(sizes)))
+    offs = [0]
+    for n in sizes:
+        offs.append(offs[-1] + n)
+    cuts = [0]
+    for g in range(1, ngroups):  # group ends where the running bytes pass g/ngroups of the batch
+        j = int(np.searchsorted(np.asarray(offs), total * g / ngroups))
+        cuts.append(min(max(j, cuts[-1] + 1), len(sizes)))
+    cuts.append(len(sizes))
+    groups = []
+    for i0, i1 in zip(cuts[:-1], cuts[1:]):
+        if i1 <= i0:
+            continue
+        gp = B.BatchCodec(sizes[i0:i1], cfg, device=dev)
+        gp.bind(ins[i0:i1], outs[i0:i1])
+        gp.compress()
+        gp.decompress()
+        gp.check()
+        ge = gp.entries_host()
+        ub = max(e.bits_offset + e.words for e in ge)
+        ug = max(e.gaps_offset + e.gap_words for e in ge)
+        groups.append({
+            "plan": gp, "a": offs[i0], "b": offs[i1], "ub": ub, "ug": ug,
+            "gc": gp.capture(compress=True, decompress=False),
+            "gd": gp.capture(compress=False, decompress=True),
+            "ent": torch.empty(gp.entries.numel(), dtype=torch.uint8, pin_memory=True),
+            "bits": torch.empty(max(ub, 1), dtype=torch.int32, pin_memory=True),
+            "gaps": torch.empty(max(ug, 1), dtype=torch.int32, pin_memory=True)})
+    in_host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+    in_host.copy_(flat)
+    out_host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+    streams = [torch.cuda.Stream(device=dev) for _ in range(max(1, args.e2e_streams))]
+
+    def e2e_step():
+        cur = torch.cuda.current_stream(dev)
+        for k, G in enumerate(groups):
+            s = streams[k % len(streams)]
+            s.wait_stream(cur)
+            gp, a_, b2, ub, ug = G["plan"], G["a"], G["b"], G["ub"], G["ug"]
+            with torch.cuda.stream(s):
+                flat[a_:b2].copy_(in_host[a_:b2], non_blocking=True)      # H2D inputs
+                G["gc"].replay()                                         # compress
+                G["ent"].copy_(gp.entries, non_blocking=True)            # D2H entries + streams
+                G["bits"][:ub].copy_(gp.bits[:ub], non_blocking=True)
+                G["gaps"][:ug].copy_(gp.gaps[:ug], non_blocking=True)
+                gp.entries.copy_(G["ent"], non_blocking=True)            # H2D for decompress
+                gp.bits[:ub].copy_(G["bits"][:ub], non_blocking=True)
+                gp.gaps[:ug].copy_(G["gaps"][:ug], non_blocking=True)
+                G["gd"].replay()                                         # decompress
+                out_host[a_:b2].copy_(flat_out[a_:b2], non_blocking=True)  # D2H outputs
+        for s in streams:
+            cur.wait_stream(s)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    e2e_steps = max(2, args.steps // 2)
+    a = torch.cuda.Event(enable_timing=True)
+    b_ = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    b_.record(stream)
+    torch.cuda.synchronize()
+    e_ms = a.elapsed_time(b_)
+    for G in groups:
+        G["plan"].check()
+    if not torch.equal(out_host, in_host):
+        raise SystemExit("e2e round trip mismatch")
+    if pg:
+        tm = torch.tensor([e_ms], device=dev)
+        pg.all_reduce(tm, op=pg.ReduceOp.MAX)
+        e_ms = float(tm.item())
+    cont = sum(G["plan"].entries.numel() + 4 * (G["ub"] + G["ug"]) for G in groups)
+    e2e = {"value": round(job_bytes * e2e_steps / e_ms / 1e6, 3), "unit": "GB/s",
+           "h2d_bytes_per_step": total + cont, "d2h_bytes_per_step": cont + total,
+           "ms_per_step": round(e_ms / e2e_steps, 3),
+           "how": f"{len(groups)} groups of consecutive buffers on {len(streams)} streams: upload, compress, "
+                  "container down and up again, decompress, download; each group's copies and "
+                  "kernels in order, groups overlapping"}
+    return e2e
+
+
 def run_batch(args, rank, world, dev, pg):
     """The batched path on the 4096-buffer workload (see the module docstring)."""
     import numpy as np
@@ -503,97 +599,11 @@ def run_batch(args, rank, world, dev, pg):
         del comp, dec_out
 
     # ---- end to end through the public API, host buffers ---------------------
-    # The batch in groups of consecutive buffers, each with its own plan and graphs, spread
-    # over a few streams: one group's uploads run while another's downloads and kernels do
-    # (PCIe is full duplex), where a single plan would copy in, compute and copy out in turn.
-    # Measured per step (groups x streams): 1 plan 150 ms, 4x2 104 ms, 8x3 95 ms, 16x4 90 ms,
-    # 32x4 89 ms -- 3.8 GB each way, ~43 GB/s per direction at once: the link, not the GPU.
     e2e = None
     if not args.no_e2e:
-        ngroups = max(1, min(args.e2e_groups, len(sizes)))
-        offs = [0]
-        for n in sizes:
-            offs.append(offs[-1] + n)
-        cuts = [0]
-        for g in range(1, ngroups):  # group ends where the running bytes pass g/ngroups of the batch
-            j = int(np.searchsorted(np.asarray(offs), total * g / ngroups))
-            cuts.append(min(max(j, cuts[-1] + 1), len(sizes)))
-        cuts.append(len(sizes))
-        groups = []
-        for i0, i1 in zip(cuts[:-1], cuts[1:]):
-            if i1 <= i0:
-                continue
-            gp = B.BatchCodec(sizes[i0:i1], cfg, device=dev)
-            gp.bind(ins[i0:i1], outs[i0:i1])
-            gp.compress()
-            gp.decompress()
-            gp.check()
-            ge = gp.entries_host()
-            ub = max(e.bits_offset + e.words for e in ge)
-            ug = max(e.gaps_offset + e.gap_words for e in ge)
-            groups.append({
-                "plan": gp, "a": offs[i0], "b": offs[i1], "ub": ub, "ug": ug,
-                "gc": gp.capture(compress=True, decompress=False),
-                "gd": gp.capture(compress=False, decompress=True),
-                "ent": torch.empty(gp.entries.numel(), dtype=torch.uint8, pin_memory=True),
-                "bits": torch.empty(max(ub, 1), dtype=torch.int32, pin_memory=True),
-                "gaps": torch.empty(max(ug, 1), dtype=torch.int32, pin_memory=True)})
-        in_host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
-        in_host.copy_(flat)
-        out_host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
-        streams = [torch.cuda.Stream(device=dev) for _ in range(max(1, args.e2e_streams))]
-
-        def e2e_step():
-            cur = torch.cuda.current_stream(dev)
-            for k, G in enumerate(groups):
-                s = streams[k % len(streams)]
-                s.wait_stream(cur)
-                gp, a_, b2, ub, ug = G["plan"], G["a"], G["b"], G["ub"], G["ug"]
-                with torch.cuda.stream(s):
-                    flat[a_:b2].copy_(in_host[a_:b2], non_blocking=True)      # H2D inputs
-                    G["gc"].replay()                                         # compress
-                    G["ent"].copy_(gp.entries, non_blocking=True)            # D2H entries + streams
-                    G["bits"][:ub].copy_(gp.bits[:ub], non_blocking=True)
-                    G["gaps"][:ug].copy_(gp.gaps[:ug], non_blocking=True)
-                    gp.entries.copy_(G["ent"], non_blocking=True)            # H2D for decompress
-                    gp.bits[:ub].copy_(G["bits"][:ub], non_blocking=True)
-                    gp.gaps[:ug].copy_(G["gaps"][:ug], non_blocking=True)
-                    G["gd"].replay()                                         # decompress
-                    out_host[a_:b2].copy_(flat_out[a_:b2], non_blocking=True)  # D2H outputs
-            for s in streams:
-                cur.wait_stream(s)
-
-        for _ in range(2):
-            e2e_step()
+        e2e = run_e2e_batch(args, sizes, flat, flat_out, ins, outs, cfg, total, job_bytes, dev, pg, stream)
         torch.cuda.synchronize()
-        if pg:
-            pg.barrier()
-        e2e_steps = max(2, args.steps // 2)
-        a = torch.cuda.Event(enable_timing=True)
-        b_ = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(e2e_steps):
-            e2e_step()
-        b_.record(stream)
-        torch.cuda.synchronize()
-        e_ms = a.elapsed_time(b_)
-        for G in groups:
-            G["plan"].check()
-        if not torch.equal(out_host, in_host):
-            raise SystemExit("e2e round trip mismatch")
-        if pg:
-            tm = torch.tensor([e_ms], device=dev)
-            pg.all_reduce(tm, op=pg.ReduceOp.MAX)
-            e_ms = float(tm.item())
-        cont = sum(G["plan"].entries.numel() + 4 * (G["ub"] + G["ug"]) for G in groups)
-        e2e = {"value": round(job_bytes * e2e_steps / e_ms / 1e6, 3), "unit": "GB/s",
-               "h2d_bytes_per_step": total + cont, "d2h_bytes_per_step": cont + total,
-               "ms_per_step": round(e_ms / e2e_steps, 3),
-               "how": f"{len(groups)} groups of consecutive buffers on {len(streams)} streams: upload, compress, "
-                      "container down and up again, decompress, download; each group's copies and "
-                      "kernels in order, groups overlapping"}
-        del groups
-        del in_host, out_host
+        torch.cuda.empty_cache()  # the serving legs start from the allocator state they had before
 
     # ---- serving: a Poisson stream of mixed requests (64 KiB .. 64 MiB) -------
     serving = None
