@@ -61,8 +61,9 @@ struct DecCfg {
     // the level-2 table stays in global memory (or the kernel parameter): codes longer
     // than the 11-bit prefix are rare, and its 5 KiB buy a fourth CTA per SM for 8 and
     // 16 stage rows (Zipf(1.2) 0.684 -> 0.592 ms, uniform bytes 0.570 -> 0.481 ms per
-    // 256 MiB); 11 rows stay at three, 32 rows at two
-    static constexpr int kMinBlocks = R == 32 ? 2 : 4;
+    // 256 MiB); 11 rows stay at three (shared memory), so they keep up to 85 registers
+    // (80 used; 1 % faster than capped at 64), 32 rows at two
+    static constexpr int kMinBlocks = R == 32 ? 2 : (R == 11 ? 3 : 4);
     static constexpr size_t kSmem = (size_t)(kT1 + kWordsPad + kGapStage) * 4 +
                                     kStageBytes + kCompactBytes + kL1Bytes;
     static_assert(kT1 % 4 == 0 && kWordsPad % 4 == 0 && kGapStage % 4 == 0 &&
