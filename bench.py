@@ -66,14 +66,20 @@ def parse():
     p.add_argument("--no-tune", action="store_true", help="skip tuning: fixed default launch shape")
     p.add_argument("--replicas", action="store_true",
                    help="N > 1: every rank runs its own whole batch (weak scaling) instead of a share of one")
-    p.add_argument("--serve-requests", type=int, default=1500,
-                   help="requests of the serving run (0: none); the full stream is 100000")
+    p.add_argument("--serve-requests", type=int, default=100000,
+                   help="requests of the serving run (0: none)")
+    p.add_argument("--serve-payloads", type=int, default=1024,
+                   help="distinct pre-encoded decompress payloads the serving requests draw from")
+    p.add_argument("--serve-overload-requests", type=int, default=5000,
+                   help="requests of the overload run (offered load above capacity, small budget)")
     p.add_argument("--serve-gbs", type=float, default=20.0, help="offered load of the serving run")
     p.add_argument("--cpu-sample-mib", type=int, default=256)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--e2e-groups", type=int, default=32, help="batched e2e: groups of consecutive buffers")
     p.add_argument("--e2e-streams", type=int, default=4, help="batched e2e: streams the groups take in turn")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-kernels", action="store_true",
+                   help="skip the single-buffer kernel timings on the plain-method inputs (C1, C2)")
     return p.parse_args()
 
 
@@ -223,6 +229,159 @@ def cpu_batch_sample(sizes, flat_host, threads: int, budget: int):
     return done, t
 
 
+# ---------------------------------------------------- plain kernels, C1 / C2 --
+PLAIN_CONFIGS = (("zipf_16m", "C1: 16 MiB i.i.d. Zipf(1.2), seed 1"),
+                 ("mixed_1g", "C2: 1 GiB of 1 MiB Zipf(1.05) / quantised N(0,1) blocks, seed 2"))
+FLUSH_BYTES = 256 << 20  # > the 126 MB L2: written before every timed repetition
+SERIAL_SAMPLE_MIB = 32   # the single-thread CPU baseline's sample
+
+
+def _median(v):
+    return round(statistics.median(v), 4)
+
+
+def _entry(ms, n, alg=None):
+    d = {"ms": _median(ms), "raw_gbs": round(n / statistics.median(ms) / 1e6, 1)}
+    if alg is not None:
+        d["alg_gbs"] = round(alg / statistics.median(ms) / 1e6, 1)
+    return d
+
+
+def time_plain_kernels(dev, reps: int = 5):
+    """This library's single-buffer entry points on the plain-method inputs
+    (C1, C2), each call bracketed by CUDA events on the launching stream, L2
+    flushed before every repetition; median of `reps`.  The operations match
+    the reference's own kernels timed by `--impl reference` (reference_gpu):
+    histogram = hgap_histogram; encode = hgap_encode given the codebook
+    (memsets, region histograms, encoder); decode = hgap_decode (workspace
+    memset, decoder); pipeline = hgap_encode_histogram + hgap_encode_prepared
+    (the histogram pass feeding the codebook, then the encoder alone)."""
+    import torch
+    import huffman_coding_gap_arrays_b200 as H
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    out = {}
+    for name, desc in PLAIN_CONFIGS:
+        x = make_workload(name, dev)
+        n = x.numel()
+        hist = H.histogram(x)
+        book, sizes = H.Codebook.from_histogram(hist.cpu())
+        enc = H.Encoder(n, dev)
+        dec = H.Decoder(sizes.segments, dev)
+        bits = torch.empty(sizes.words + 4, dtype=torch.int32, device=dev)
+        gaps = torch.empty(sizes.gap_words + 4, dtype=torch.int32, device=dev)
+        y = torch.empty(n, dtype=torch.uint8, device=dev)
+        C = 4 * (sizes.words + sizes.gap_words)
+        t = {k: [] for k in ("histogram", "encode", "decode", "pass1", "encode_kernel")}
+
+        def timed(key, fn):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            t[key].append(a.elapsed_time(b))
+
+        for r in range(reps + 1):
+            timed("histogram", lambda: H.histogram(x, out=hist))
+            timed("encode", lambda: enc.encode(x, book, sizes, bits=bits, gaps=gaps, check_status=False))
+            timed("decode", lambda: dec.decode(bits[:sizes.words], gaps[:sizes.gap_words], sizes, book, n,
+                                               out=y, check_status=False))
+            timed("pass1", lambda: enc.histogram(x, out=hist))
+            timed("encode_kernel", lambda: enc.encode(x, book, sizes, bits=bits, gaps=gaps, check_status=False,
+                                                      prepared=True))
+            if r == 0:
+                for v in t.values():
+                    v.clear()  # the first round is a warm-up
+        enc.check()
+        dec.decode(bits[:sizes.words], gaps[:sizes.gap_words], sizes, book, n, out=y)
+        if not torch.equal(y, x):
+            raise SystemExit(f"{name}: decode(encode(x)) != x")
+        out[name] = {
+            "config": desc, "bytes": n, "compressed_bytes": C,
+            "histogram": _entry(t["histogram"], n, n),
+            "encode": _entry(t["encode"], n, 2 * n + C),
+            "decode": _entry(t["decode"], n, C + n),
+            "pipeline_pass1": _entry(t["pass1"], n, n),
+            "pipeline_encode_kernel": _entry(t["encode_kernel"], n, n + C),
+        }
+        del x, bits, gaps, y, enc, dec
+        torch.cuda.empty_cache()
+    return out
+
+
+def time_reference_kernels(dev, reps: int = 5):
+    """The reference's OWN GPU kernels (encoder/src/encoder.cu,
+    decoder/src/decoder.cu, built unmodified for sm_100a into oracle/_ref) on
+    the same plain-method inputs and with the same timing rules as
+    time_plain_kernels: cu_histgram + mergeHistogram; encode() on the device
+    (its memsets, cuencoder, cu_get_gaparray) given the reference's own
+    codebook; decoder_l1_l2() on the device (its memsets, gpu_dec_l1_l2).  The
+    reference decoder's output is checked against the input."""
+    import numpy as np
+    import torch
+    from oracle import oracle as O
+    from oracle import ref_gpu as RG
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    out = {}
+    for name, desc in PLAIN_CONFIGS:
+        x = make_workload(name, dev)
+        n = x.numel()
+        buf = RG.padded_input(x, dev)
+        h, _, _ = RG.histogram(buf, n)
+        cb = O.ref_codebook(h)
+        _, W, S, G = cb.sizes()
+        C = 4 * (W + G)
+        t = {k: [] for k in ("hist", "merge", "enc_memset", "cuencoder", "gaparray", "dec_memset", "gpu_dec")}
+        dbufs = None
+        decoded = None
+        for r in range(reps + 1):
+            flush.zero_()
+            _, a, b = RG.histogram(buf, n)
+            t["hist"].append(a)
+            t["merge"].append(b)
+            flush.zero_()
+            bits, gaps, m, e, g = RG.encode(buf, n, cb)
+            t["enc_memset"].append(m)
+            t["cuencoder"].append(e)
+            t["gaparray"].append(g)
+            if dbufs is None:
+                dbufs = RG.DecodeBuffers(bits, gaps, n)
+            flush.zero_()
+            res = RG.decode(dbufs, S, cb)
+            if res is not None:
+                decoded, m, k = res
+                t["dec_memset"].append(m)
+                t["gpu_dec"].append(k)
+            if r == 0:
+                for v in t.values():
+                    v.clear()
+        torch.cuda.synchronize()
+        entry = {"config": desc, "bytes": n, "compressed_bytes": C,
+                 "histogram": _entry([a + b for a, b in zip(t["hist"], t["merge"])], n, n),
+                 "histogram_kernels_ms": {"cu_histgram": _median(t["hist"]), "mergeHistogram": _median(t["merge"])},
+                 "encode": _entry([a + b + c for a, b, c in zip(t["enc_memset"], t["cuencoder"], t["gaparray"])],
+                                  n, n + C),
+                 "encode_kernels_ms": {"memsets": _median(t["enc_memset"]), "cuencoder": _median(t["cuencoder"]),
+                                       "cu_get_gaparray": _median(t["gaparray"])}}
+        if t["gpu_dec"]:
+            entry["decode"] = _entry([a + b for a, b in zip(t["dec_memset"], t["gpu_dec"])], n, C + n)
+            entry["decode_kernels_ms"] = {"memsets": _median(t["dec_memset"]), "gpu_dec_l1_l2": _median(t["gpu_dec"])}
+            entry["decode_round_trip_exact"] = bool(torch.equal(decoded, x))
+        else:
+            entry["decode"] = None
+            entry["decode_skipped"] = "the reference's level-1 table boundary is wrong for this codebook"
+        ref_bits = np.asarray(bits.cpu().numpy()).view(np.uint32)
+        entry["stream_words"] = int(ref_bits.size)
+        out[name] = entry
+        del x, buf, bits, gaps, dbufs, decoded
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, rank: int, world: int):
     """`--impl reference`: the reference path's CPU implementation (the oracle
     port -- the reference itself has no CPU encoder/decoder) on the box's host
@@ -264,6 +423,18 @@ def run_reference(args, rank: int, world: int):
         value = sample * args.steps / t / 1e9
         what = (f"first {sample >> 20} MiB of the workload, histogram+codebook+encode+decode per step "
                 f"(oracle/hgap_oracle.c, pthreads)")
+    ref_gpu = None
+    if not args.no_kernels:
+        from oracle import ref_gpu as RG
+        if not torch.cuda.is_available():
+            ref_gpu = {"unavailable": "no CUDA device"}
+        elif not RG.available():
+            ref_gpu = {"unavailable": "oracle/_ref/libref_gpu_time.so not built (reference sources absent)"}
+        else:
+            ref_gpu = time_reference_kernels(torch.device("cuda", 0))
+            ref_gpu["how"] = ("the reference's own kernels (encoder/src/encoder.cu, decoder/src/decoder.cu, "
+                              "unmodified, sm_100a) launched as its histgram()/encode()/decoder_l1_l2() do, "
+                              "CUDA events around each, L2 flushed before each repetition, median of 5")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GB/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -274,6 +445,7 @@ def run_reference(args, rank: int, world: int):
                          "sample": what},
         "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "reference_gpu": ref_gpu,
     }
     print(json.dumps(line), flush=True)
     del torch
@@ -319,34 +491,55 @@ def picks_cfg(tuning):
 def run_serving(args, pool, learned, fixed_cfg, dev):
     """Serving at `--serve-gbs` offered load: the learned tuner, the one shape
     the exhaustive search chose for the batched workload, and the plain
-    per-request path, each on the same request stream."""
+    per-request path, each on the same request stream; then one run at an
+    offered load far above capacity with a small HBM budget, so that the
+    admission control binds.  Decompress requests draw from a pool of
+    `--serve-payloads` streams, each a buffer of the batched workload's
+    distributions (Zipf or quantised Gaussian by its seed) with a size
+    log-uniform in [64 KiB, 64 MiB], encoded by the batched path."""
     import numpy as np
     import torch
     from huffman_coding_gap_arrays_b200 import serve as SV
-    from huffman_coding_gap_arrays_b200 import tuner as T
+    from huffman_coding_gap_arrays_b200 import workloads as WL
     rng = np.random.default_rng(17)
-    bufs = []
-    for _ in range(32):  # decompress payloads: slices of the pool, pre-encoded
-        n = int(np.exp(rng.uniform(np.log(64 << 10), np.log(64 << 20))))
-        off = int(rng.integers(0, pool.numel() - n))
-        bufs.append(pool[off:off + n])
-    streams = SV.encode_streams(bufs)
-    traffic = T.batch_features(bufs)[1:]
+    streams = []
+    for k0 in range(0, args.serve_payloads, 128):  # encoded 128 at a time: the raw buffers go after
+        bufs = [WL.batch_buffer(int(np.exp(rng.uniform(np.log(64 << 10), np.log(64 << 20)))), 500_000 + k, dev)
+                for k in range(k0, min(args.serve_payloads, k0 + 128))]
+        streams += SV.encode_streams(bufs)
+        del bufs
+    torch.cuda.synchronize()
+    traffic = np.mean([st.features for st in streams], axis=0)
     out = {"requests": args.serve_requests, "offered_gbs": args.serve_gbs, "hbm_budget_gb": 40,
            "sizes": "log-uniform 64 KiB .. 64 MiB, 50/50 compress/decompress, Poisson arrivals",
-           "warmup": "an untimed stream of a fifth as many requests first, per policy",
-           "where": "payloads and results resident in HBM; latency = queueing + GPU service"}
+           "payloads": f"compress: slices of the batched workload; decompress: one of {len(streams)} "
+                       f"pre-encoded streams of its distributions, drawn per request",
+           "warmup": "an untimed stream of min(5000, a fifth) as many requests first, per policy",
+           "where": "payloads and results resident in HBM; latency = queueing + GPU service; "
+                    "service = launch to completion"}
     policies = [("autotuner_fixed", dict(config=fixed_cfg))]
     if learned is not None and learned.usable:
         policies.insert(0, ("mlp", dict(tuner=learned)))
     policies.append(("plain", dict(policy="plain")))
+    warm = min(5000, max(100, args.serve_requests // 5))
     for name, kw in policies:
         srv = SV.Server(hbm_budget=40e9, traffic_features=traffic, device=dev, **kw)
         # untimed warm-up stream: the allocator's pools and the launch attributes settle first
-        srv.run(SV.poisson_requests(max(100, args.serve_requests // 5), args.serve_gbs, pool, streams, seed=29))
-        srv.batches, srv.peak_held = 0, 0
+        srv.run(SV.poisson_requests(warm, args.serve_gbs, pool, streams, seed=29))
+        srv.reset_counters()
         reqs = SV.poisson_requests(args.serve_requests, args.serve_gbs, pool, streams, seed=23)
         out[name] = srv.run(reqs)
+        del reqs
+        torch.cuda.synchronize()
+    if args.serve_overload_requests:
+        gbs, budget = 400.0, 4e9
+        srv = SV.Server(hbm_budget=budget, traffic_features=traffic, device=dev, config=fixed_cfg)
+        srv.run(SV.poisson_requests(min(1000, args.serve_overload_requests), gbs, pool, streams, seed=31))
+        srv.reset_counters()
+        reqs = SV.poisson_requests(args.serve_overload_requests, gbs, pool, streams, seed=37)
+        st = srv.run(reqs)
+        st["offered_gbs"] = gbs
+        out["overload_autotuner_fixed"] = st
         del reqs
         torch.cuda.synchronize()
     return out
@@ -607,7 +800,7 @@ def run_batch(args, rank, world, dev, pg):
 
     # ---- serving: a Poisson stream of mixed requests (64 KiB .. 64 MiB) -------
     serving = None
-    if args.serve_requests and rank == 0:
+    if args.serve_requests and rank == 0 and world == 1:
         serving = run_serving(args, flat, learned, picks_cfg(tuning), dev)
 
     cpu = None
@@ -620,6 +813,17 @@ def run_batch(args, rank, world, dev, pg):
         cpu = {"value": round(done / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                "sample": f"the batch's first buffers up to {budget >> 20} MiB ({done} bytes), one "
                          f"histogram+codebook+encode+decode round trip per buffer (oracle/hgap_oracle.c, pthreads)"}
+        sb = SERIAL_SAMPLE_MIB << 20
+        done1, dt1 = cpu_batch_sample(sizes, fh, 1, sb)
+        cpu["serial"] = {"value": round(done1 / dt1 / 1e9, 4), "unit": "GB/s", "cores": 1,
+                         "sample": f"the batch's first buffers up to {SERIAL_SAMPLE_MIB} MiB ({done1} bytes), "
+                                   f"the same round trip on one thread"}
+
+    plain_kernels = None
+    if rank == 0 and world == 1 and not args.no_kernels:
+        plain_kernels = time_plain_kernels(dev)
+        plain_kernels["how"] = ("hgap_histogram / hgap_encode / hgap_decode and the two-call pipeline, CUDA "
+                                "events around each call, L2 flushed before each repetition, median of 5")
 
     if rank == 0:
         value = job_bytes * args.steps / ms / 1e6
@@ -647,6 +851,7 @@ def run_batch(args, rank, world, dev, pg):
             "speedup_vs_plain": (round(value / world / plain["roundtrip_gbs"], 2)
                                  if plain else None),
             "kernels": kernels,
+            "plain_kernels": plain_kernels,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -840,6 +1045,11 @@ def main():
         cpu = {"value": round(sample / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                "sample": f"first {sample >> 20} MiB of the workload, one histogram+codebook+encode+"
                          f"decode round trip (oracle/hgap_oracle.c, pthreads)"}
+        s1 = min(n, SERIAL_SAMPLE_MIB << 20)
+        dt1, y1 = cpu_roundtrip(np.ascontiguousarray(xs[:s1]), 1)
+        assert np.array_equal(y1, xs[:s1])
+        cpu["serial"] = {"value": round(s1 / dt1 / 1e9, 4), "unit": "GB/s", "cores": 1,
+                         "sample": f"first {s1 >> 20} MiB of the workload, the same round trip on one thread"}
 
     if rank == 0:
         line = {

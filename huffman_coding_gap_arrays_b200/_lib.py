@@ -30,7 +30,7 @@ EXPORTS = [
     "hgap_decode_table_build", "hgap_decode_table_build_device", "hgap_batch_compress_workspace_bytes",
     "hgap_batch_decompress_workspace_bytes", "hgap_batch_bits_capacity", "hgap_batch_gaps_capacity",
     "hgap_batch_compress", "hgap_batch_decompress", "hgap_batch_status", "hgap_mlp_forward",
-    "hgap_mlp_loss_grad", "hgap_mlp_adam",
+    "hgap_mlp_loss_grad", "hgap_mlp_adam", "hgap_encode_hold", "hgap_decode_hold",
 ]
 
 
@@ -108,6 +108,8 @@ def lib() -> C.CDLL:
     L.hgap_decode_workspace_bytes.restype = C.c_size_t
     L.hgap_decode.argtypes = [vp, u64, vp, u64, C.POINTER(CCodebook), vp, u64, vp, C.c_size_t, vp]
     L.hgap_workspace_status.argtypes = [vp, vp]
+    L.hgap_encode_hold.argtypes = L.hgap_encode.argtypes + [u64, u64]
+    L.hgap_decode_hold.argtypes = L.hgap_decode.argtypes + [u64, u64]
     L.hgap_decode_noalloc.argtypes = [vp, u64, vp, u64, C.POINTER(CCodebook), vp, u64, vp]
     L.hgap_container_bytes.argtypes = [C.c_uint32, u64, u64]
     L.hgap_container_bytes.restype = C.c_size_t

@@ -51,7 +51,7 @@ def _upload(values, dtype, out: torch.Tensor | None = None, device=None) -> torc
     """Host values to the device through pinned memory, ordered on the current
     stream without blocking the host (a pageable copy would wait for the
     stream's earlier work)."""
-    host = torch.as_tensor(np.asarray(values), dtype=dtype).pin_memory()
+    host = torch.tensor(np.array(values, copy=True), dtype=dtype).pin_memory()
     if out is None:
         return host.to(device, non_blocking=True)
     out.copy_(host, non_blocking=True)
@@ -62,7 +62,7 @@ class BatchCodec:
     """Workspaces, arenas and pointer tables for a fixed list of buffer sizes."""
 
     def __init__(self, sizes, config: LaunchConfig | None = None, device=None,
-                 region_chunks: np.ndarray | None = None):
+                 region_chunks: np.ndarray | None = None, decompress: bool = True):
         self.sizes = np.ascontiguousarray(np.asarray(sizes, dtype=np.uint64))
         self.count = int(self.sizes.size)
         self.config = config or LaunchConfig()
@@ -70,7 +70,8 @@ class BatchCodec:
         L = lib()
         cfg = self.config.cstruct()
         enc_ws = L.hgap_batch_compress_workspace_bytes(self.count, _u64p(self.sizes), C.byref(cfg))
-        dec_ws = L.hgap_batch_decompress_workspace_bytes(self.count, _u64p(self.sizes))
+        # a compress-only plan (decompress=False) holds no decompress workspace
+        dec_ws = L.hgap_batch_decompress_workspace_bytes(self.count, _u64p(self.sizes)) if decompress else 8
         self.bits_capacity = int(L.hgap_batch_bits_capacity(self.count, _u64p(self.sizes)))
         self.gaps_capacity = int(L.hgap_batch_gaps_capacity(self.count, _u64p(self.sizes)))
         dev = self.device

@@ -24,7 +24,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-Wall",
 
 SOURCES = ["hist.cu", "encode.cu", "decode.cu", "api.cu", "batch.cu", "mlp.cu", "compat.cu", "noalloc.cu",
            "host.cpp"]
-HEADERS = ["hgap_internal.h", "device_util.cuh", "book.cuh", "dec_entry.cuh"]
+HEADERS = ["hgap_internal.h", "device_util.cuh", "book.cuh", "dec_entry.cuh", "launch_cache.h"]
 
 
 def _newer(target: str, deps) -> bool:

@@ -172,9 +172,13 @@ hgap_status hgap_encode_part_prepared(const void* d_in, uint64_t n, const hgap_c
     return cuda_status(hgap::launch_encode(a, t, 0, stream));
 }
 
-hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
-                        uint64_t words, uint32_t* d_gaps, uint64_t segments, void* d_workspace,
-                        size_t workspace_bytes, hgap_stream_t stream) {
+}  // extern "C"
+
+namespace {
+
+hgap_status encode_impl(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits, uint64_t words,
+                        uint32_t* d_gaps, uint64_t segments, void* d_workspace, size_t workspace_bytes,
+                        hgap_stream_t stream, const hgap::LookbackHook& hook) {
     if (!cb) return HGAP_ERR_INVALID_ARG;
     if (n == 0) return (words == 0 && segments == 0) ? HGAP_OK : HGAP_ERR_SIZE;
     hgap::EncArgs a;
@@ -190,16 +194,13 @@ hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, u
     // per-region histograms into the workspace (the scratch histogram was cleared with the header)
     int e = hgap::launch_hist_st(h, 0, stream);
     if (e != 0) return HGAP_ERR_CUDA;
+    a.hook = hook;
     return cuda_status(hgap::launch_encode(a, t, 0, stream));
 }
 
-size_t hgap_decode_workspace_bytes(uint64_t segments) {
-    return kWsHeader + sizeof(uint64_t) * (size_t)hgap::decode_tiles(segments, 1);  // worst case
-}
-
-hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps,
-                        uint64_t segments, const hgap_codebook* cb, uint8_t* d_out, uint64_t n,
-                        void* d_workspace, size_t workspace_bytes, hgap_stream_t stream) {
+hgap_status decode_impl(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps, uint64_t segments,
+                        const hgap_codebook* cb, uint8_t* d_out, uint64_t n, void* d_workspace,
+                        size_t workspace_bytes, hgap_stream_t stream, const hgap::LookbackHook& hook) {
     if (!cb) return HGAP_ERR_INVALID_ARG;
     if (n == 0) return (words == 0 && segments == 0) ? HGAP_OK : HGAP_ERR_SIZE;
     if (!d_bits || !d_gaps || !d_out || !d_workspace) return HGAP_ERR_INVALID_ARG;
@@ -247,7 +248,52 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     const bool complete = kraft == (1ull << hgap::kMaxLen);
     // two symbols per lookup pay off once about a third of the lookups yield two
     const bool pairs = hgap::dec_pair_fraction(t) >= 0.3;
+    a.hook = hook;
     return cuda_status(hgap::launch_decode(a, t, min_len, complete, pairs, 0, stream));
+}
+
+hgap::LookbackHook hold_hook(uint64_t hold, uint64_t wait_limit_ns) {
+    hgap::LookbackHook h;
+    h.hold_plus1 = hold == ~0ull ? 0 : hold + 1;
+    h.wait_ns = wait_limit_ns;
+    return h;
+}
+
+}  // namespace
+
+extern "C" {
+
+hgap_status hgap_encode(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
+                        uint64_t words, uint32_t* d_gaps, uint64_t segments, void* d_workspace,
+                        size_t workspace_bytes, hgap_stream_t stream) {
+    return encode_impl(d_in, n, cb, d_bits, words, d_gaps, segments, d_workspace, workspace_bytes, stream,
+                       hgap::LookbackHook{0, 0});
+}
+
+hgap_status hgap_encode_hold(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
+                             uint64_t words, uint32_t* d_gaps, uint64_t segments, void* d_workspace,
+                             size_t workspace_bytes, hgap_stream_t stream, uint64_t hold, uint64_t wait_limit_ns) {
+    return encode_impl(d_in, n, cb, d_bits, words, d_gaps, segments, d_workspace, workspace_bytes, stream,
+                       hold_hook(hold, wait_limit_ns));
+}
+
+size_t hgap_decode_workspace_bytes(uint64_t segments) {
+    return kWsHeader + sizeof(uint64_t) * (size_t)hgap::decode_tiles(segments, 1);  // worst case
+}
+
+hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps,
+                        uint64_t segments, const hgap_codebook* cb, uint8_t* d_out, uint64_t n,
+                        void* d_workspace, size_t workspace_bytes, hgap_stream_t stream) {
+    return decode_impl(d_bits, words, d_gaps, segments, cb, d_out, n, d_workspace, workspace_bytes, stream,
+                       hgap::LookbackHook{0, 0});
+}
+
+hgap_status hgap_decode_hold(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps,
+                             uint64_t segments, const hgap_codebook* cb, uint8_t* d_out, uint64_t n,
+                             void* d_workspace, size_t workspace_bytes, hgap_stream_t stream, uint64_t hold,
+                             uint64_t wait_limit_ns) {
+    return decode_impl(d_bits, words, d_gaps, segments, cb, d_out, n, d_workspace, workspace_bytes, stream,
+                       hold_hook(hold, wait_limit_ns));
 }
 
 hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream) {

@@ -28,6 +28,7 @@
 
 #include "dec_entry.cuh"
 #include "device_util.cuh"
+#include "launch_cache.h"
 
 namespace hgap {
 
@@ -351,12 +352,14 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
         const uint32_t before1 = warp ? __shfl_sync(kFull, w1, warp - 1) : 0u;
         const uint32_t Ct = total0 + total1;
         const uint32_t excl[2] = {before0 + i0 - n[0], total0 + before1 + i1 - n[1]};
-        if (tid == 0 && have) lookback_publish(a.lookback, T.job.item0 + T.local, Ct, T.local == 0);
+        if (tid == 0 && have && T.job.item0 + T.local + 1 != a.hook.hold_plus1)
+            lookback_publish(a.lookback, T.job.item0 + T.local, Ct, T.local == 0);
         if (have_next) HGAP_PREFETCH(ns);  // in flight while prev is resolved and written
         if (prev_s >= 0 && warp == 0) {
             const DecSlot& Pv = slot[prev_s];
-            const uint64_t O =
-                lookback_resolve<kDecLookK>(a.lookback, Pv.job.item0 + Pv.local, prev_ct, Pv.local == 0, a.status, lane);
+            const uint64_t rec = Pv.job.item0 + Pv.local;
+            const uint64_t O = lookback_resolve<kDecLookK>(a.lookback, rec, prev_ct, Pv.local == 0, a.status, lane,
+                                                           wait_limit(a.hook), rec + 1 != a.hook.hold_plus1);
             if (lane == 0) s_O = O;
         }
         __syncthreads();  // (3) prev's output offset known
@@ -458,16 +461,10 @@ template <int R, bool COMPLETE, bool PAIRS>
 static int launch_decode_r(const DecArgs& a, const DecTable& t, int ctas_per_sm, cudaStream_t st) {
     using C = DecCfg<R>;
     auto kern = decode_kernel<R, COMPLETE, PAIRS>;
-    static int sms = 0, per_sm = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::kSmem);
-        if (e != cudaSuccess) return e;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kDecThreads, C::kSmem);
-        if (per_sm < 1) per_sm = 1;
-    }
+    static LaunchCache cache;  // one per kernel instantiation
+    const LaunchFacts f = cache.get(reinterpret_cast<const void*>(kern), kDecThreads, C::kSmem);
+    if (f.err != cudaSuccess) return f.err;
+    const int sms = f.sms, per_sm = f.per_sm;
     const int k = (ctas_per_sm > 0 && ctas_per_sm < per_sm) ? ctas_per_sm : per_sm;
     const uint64_t cap = (uint64_t)sms * k;
     const unsigned grid = (unsigned)(a.nitems_dev ? cap : (a.nitems < cap ? (a.nitems ? a.nitems : 1) : cap));

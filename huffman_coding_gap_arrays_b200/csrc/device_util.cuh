@@ -49,11 +49,14 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
     return t;
 }
 
-// Waits until *p != 0 and returns it.  Bounded: after kWaitLimitNs, or as
-// soon as any error is already flagged, it flags kDevTimeout and returns
-// `fallback`, so the caller finishes its tile and the kernel exits.
-__device__ __forceinline__ uint64_t wait_nonzero(const uint64_t* p, uint32_t* status,
-                                                 uint64_t fallback) {
+// Waits until *p != 0 and returns it.  Bounded: once `limit_ns` of
+// %globaltimer have passed it flags kDevTimeout and returns `fallback`, so the
+// caller finishes its tile and the kernel exits.  If another error is already
+// flagged (a corrupt stream, a missing codeword, ...) it returns `fallback` at
+// once without flagging a timeout: the output is void anyway, and the status
+// word then names the real cause, whatever the timing.
+__device__ __forceinline__ uint64_t wait_nonzero(const uint64_t* p, uint32_t* status, uint64_t fallback,
+                                                 uint64_t limit_ns) {
     uint64_t v = ld_relaxed_u64(p);
     if (v != 0) return v;
     const uint64_t t0 = global_timer_ns();
@@ -61,7 +64,8 @@ __device__ __forceinline__ uint64_t wait_nonzero(const uint64_t* p, uint32_t* st
         v = ld_relaxed_u64(p);
         if (v != 0) return v;
         if ((it & 31) == 0) {
-            if (ld_relaxed_u32(status) != 0 || global_timer_ns() - t0 > kWaitLimitNs) {
+            if (ld_relaxed_u32(status) != 0) return fallback;
+            if (global_timer_ns() - t0 > limit_ns) {
                 atomicOr(status, kDevTimeout);
                 return fallback;
             }
@@ -129,6 +133,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
     }
 }
 
+// The wait limit of a launch's look-back waits (the test hook may shorten it).
+__device__ __forceinline__ uint64_t wait_limit(const LookbackHook& h) {
+    return h.wait_ns ? h.wait_ns : kWaitLimitNs;
+}
+
 // The job owning global work item `it`: the largest j with item0s[j] <= it
 // (item0s ascends, item0s[count] is the total; empty jobs are skipped).
 __device__ __forceinline__ uint32_t find_job(const uint64_t* item0s, uint32_t count, uint64_t it) {
@@ -157,34 +166,8 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, uint32_t lane) {
 }
 
 // Single-pass decoupled look-back (the reference's scheme,
-// encoder/src/encoder.cu:222-263, decoder/src/decoder.cu:601-638), run by one
-// full warp: publishes the tile aggregate, then inspects 32 predecessors per
-// step, nearest first, until one carries an inclusive prefix.  Every wait is
-// bounded.  Returns the exclusive prefix of `tile` to all lanes and publishes
-// its inclusive prefix.
-__device__ __forceinline__ uint64_t lookback_warp(uint64_t* rec, uint64_t tile, uint64_t agg,
-                                                  uint32_t* status, uint32_t lane) {
-    if (tile == 0) {
-        if (lane == 0) st_relaxed_u64(rec, kFlagP | agg);
-        return 0;
-    }
-    if (lane == 0) st_relaxed_u64(rec + tile, kFlagA | agg);
-    uint64_t excl = 0;
-    int64_t idx = (int64_t)tile - 1 - (int64_t)lane;
-    for (;;) {
-        const uint64_t v = idx >= 0 ? wait_nonzero(rec + idx, status, kFlagP) : kFlagP;
-        const uint32_t pmask = __ballot_sync(kFull, (v & kFlagP) != 0);
-        uint64_t val = v & kValueMask;
-        if (pmask != 0 && lane > (uint32_t)(__ffs(pmask) - 1)) val = 0;
-        excl += warp_sum_u64(val);
-        if (pmask != 0) break;
-        idx -= 32;
-    }
-    if (lane == 0) st_relaxed_u64(rec + tile, kFlagP | ((excl + agg) & kValueMask));
-    return excl;
-}
-
-// The same look-back with a window of 32*K predecessors per round trip: lane
+// encoder/src/encoder.cu:222-263, decoder/src/decoder.cu:601-638) run by one
+// full warp, with a window of 32*K predecessors per round trip: lane
 // l holds tiles top-K*l ... top-K*l-K+1 (nearest first, window position
 // K*l + j).  The inclusive-prefix frontier advances at most one window per L2
 // round trip, so the window must exceed the tiles started per round trip.
@@ -202,9 +185,12 @@ __device__ __forceinline__ void lookback_publish(uint64_t* rec, uint64_t tile, u
     st_relaxed_u64(rec + tile, (first ? kFlagP : kFlagA) | (agg & kValueMask));
 }
 
+// `limit_ns` bounds each wait; `publish` = false keeps the inclusive prefix
+// unpublished (the bounded-wait test hook only: LookbackHook).
 template <int K>
 __device__ __forceinline__ uint64_t lookback_resolve(uint64_t* rec, uint64_t tile, uint64_t agg, bool first,
-                                                     uint32_t* status, uint32_t lane) {
+                                                     uint32_t* status, uint32_t lane, uint64_t limit_ns,
+                                                     bool publish = true) {
     if (first) return 0;
     uint64_t excl = 0;
     int64_t top = (int64_t)tile - 1;
@@ -230,10 +216,10 @@ __device__ __forceinline__ uint64_t lookback_resolve(uint64_t* rec, uint64_t til
         if (gz < gp) {  // an unpublished record in front of the nearest inclusive prefix
             if ((int)lane == lz) {
                 const int64_t i = top - (int64_t)gz;
-                wait_nonzero(rec + i, status, kFlagP);
+                wait_nonzero(rec + i, status, kFlagP, limit_ns);
             }
             __syncwarp();
-            if (ld_relaxed_u32(status) & kDevTimeout) return excl;  // gave up: the status says so
+            if (ld_relaxed_u32(status) != 0) return excl;  // gave up, or the output is void: the status says so
             continue;  // reload the same window
         }
         uint64_t sum = 0;
@@ -244,7 +230,7 @@ __device__ __forceinline__ uint64_t lookback_resolve(uint64_t* rec, uint64_t til
         if (gp < 32 * K) break;
         top -= 32 * K;
     }
-    if (lane == 0) st_relaxed_u64(rec + tile, kFlagP | ((excl + agg) & kValueMask));
+    if (lane == 0 && publish) st_relaxed_u64(rec + tile, kFlagP | ((excl + agg) & kValueMask));
     return excl;
 }
 

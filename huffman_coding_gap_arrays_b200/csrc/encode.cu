@@ -46,6 +46,7 @@
 #include <cuda_runtime.h>
 
 #include "device_util.cuh"
+#include "launch_cache.h"
 
 namespace hgap {
 
@@ -110,7 +111,7 @@ __device__ __forceinline__ void claim_region(const EncArgs& a, const uint32_t* l
             part += (uint64_t)a.st_hist[item * 256 + b] * len;
         }
         agg = warp_sum_u64(part);
-        if (lane == 0) lookback_publish(a.st_rec, item, agg, item == src->item0);
+        if (lane == 0 && item + 1 != a.hook.hold_plus1) lookback_publish(a.st_rec, item, agg, item == src->item0);
     }
     if (lane == 0) {
         sh.item[slot] = item;
@@ -219,7 +220,8 @@ __global__ void __launch_bounds__(kEncThreads, 2)
         // ---- warp 0: G of the current region, bits before G ---------------------
         if (warp == 0) {
             const uint64_t G =
-                J.bit0 + lookback_resolve<4>(a.st_rec, item, sh.agg[cur_slot], st == 0, a.status, lane);
+                J.bit0 + lookback_resolve<4>(a.st_rec, item, sh.agg[cur_slot], st == 0, a.status, lane,
+                                             wait_limit(a.hook), item + 1 != a.hook.hold_plus1);
             uint32_t head = 0, gcarry = 0;
             const uint32_t r = (uint32_t)(G & 31);
             const uint32_t nibs = (uint32_t)((G >> 7) & 7);
@@ -456,17 +458,10 @@ __global__ void __launch_bounds__(kEncThreads, 2)
 // ------------------------------------------------------------- launchers ---
 
 int launch_encode(const EncArgs& a, const EncTable& t, int ctas_per_sm, void* stream) {
-    static int sms = 0, per_sm = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaError_t e = cudaFuncSetAttribute(encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kEncSmem);
-        if (e != cudaSuccess) return e;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, encode_kernel, kEncThreads, kEncSmem);
-        if (per_sm < 1) per_sm = 1;
-    }
+    static LaunchCache cache;
+    const LaunchFacts f = cache.get(reinterpret_cast<const void*>(encode_kernel), kEncThreads, kEncSmem);
+    if (f.err != cudaSuccess) return f.err;
+    const int sms = f.sms, per_sm = f.per_sm;
     const int k = (ctas_per_sm > 0 && ctas_per_sm < per_sm) ? ctas_per_sm : per_sm;
     const uint64_t cap = (uint64_t)sms * k;
     const unsigned grid = (unsigned)(a.nitems_dev ? cap : (a.nitems < cap ? (a.nitems ? a.nitems : 1) : cap));

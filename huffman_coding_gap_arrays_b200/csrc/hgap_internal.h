@@ -38,6 +38,15 @@ constexpr uint64_t kValueMask = ~kFlagMask;
 // Hand-off record: valid bit over a 32-bit payload.
 constexpr uint64_t kHandValid = 1ull << 32;
 
+// Bounded-wait test hook, all zero in every product call: the work item
+// (encoder region / decoder tile, in the launch's numbering) plus one whose
+// look-back records are never published, and the limit of every look-back
+// wait in ns (0: the default, kWaitLimitNs).
+struct LookbackHook {
+    uint64_t hold_plus1;
+    uint64_t wait_ns;
+};
+
 // Workspace header (both kernels): status word, tile counter, padding.
 constexpr size_t kWsHeader = 256;
 
@@ -113,6 +122,7 @@ struct EncArgs {
     const uint64_t* tag;        // single path: {n, input address} written by the histogram pass
     uint32_t* counter;
     uint32_t* status;
+    LookbackHook hook;
 };
 
 struct HistStArgs {
@@ -199,6 +209,7 @@ struct DecArgs {
     uint64_t* lookback;
     uint32_t* counter;
     uint32_t* status;
+    LookbackHook hook;
 };
 
 // --------------------------------------------------------------- launchers --

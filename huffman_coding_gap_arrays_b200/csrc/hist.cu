@@ -12,24 +12,31 @@
 #include <cuda_runtime.h>
 
 #include "device_util.cuh"
+#include "launch_cache.h"
 
 namespace hgap {
 
 constexpr int kHistThreads = 512;
 constexpr int kHistUnroll = 4;
 
-__device__ __forceinline__ void hist_word(uint32_t* hl, uint32_t w) {
-    atomicAdd(hl + ((w << 5) & 0x1fe0u), 1u);
-    atomicAdd(hl + ((w >> 3) & 0x1fe0u), 1u);
-    atomicAdd(hl + ((w >> 11) & 0x1fe0u), 1u);
-    atomicAdd(hl + ((w >> 19) & 0x1fe0u), 1u);
+// Byte b counts at h[b * 32 + lane], byte offset (b << 7) | (lane << 2): one
+// shift and one and-or (lane4 = lane << 2) per byte, then the shared atomic.
+__device__ __forceinline__ void hist_add(uint32_t* h, uint32_t off) {
+    atomicAdd(reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(h) + off), 1u);
 }
 
-__device__ __forceinline__ void hist_chunk(uint32_t* hl, const uint4 v) {
-    hist_word(hl, v.x);
-    hist_word(hl, v.y);
-    hist_word(hl, v.z);
-    hist_word(hl, v.w);
+__device__ __forceinline__ void hist_word(uint32_t* h, uint32_t lane4, uint32_t w) {
+    hist_add(h, ((w << 7) & 0x7f80u) | lane4);
+    hist_add(h, ((w >> 1) & 0x7f80u) | lane4);
+    hist_add(h, ((w >> 9) & 0x7f80u) | lane4);
+    hist_add(h, ((w >> 17) & 0x7f80u) | lane4);
+}
+
+__device__ __forceinline__ void hist_chunk(uint32_t* h, uint32_t lane4, const uint4 v) {
+    hist_word(h, lane4, v.x);
+    hist_word(h, lane4, v.y);
+    hist_word(h, lane4, v.z);
+    hist_word(h, lane4, v.w);
 }
 
 __global__ void __launch_bounds__(kHistThreads, 4)
@@ -38,7 +45,7 @@ __global__ void __launch_bounds__(kHistThreads, 4)
     __shared__ uint32_t h[256 * 32];
     for (int i = threadIdx.x; i < 256 * 32; i += kHistThreads) h[i] = 0;
     __syncthreads();
-    uint32_t* hl = h + (threadIdx.x & 31);
+    const uint32_t lane4 = (threadIdx.x & 31) << 2;
 
     const uint64_t first_full = (lo + 15) >> 4;  // chunks wholly inside [lo, hi)
     const uint64_t end_full = hi >> 4;
@@ -49,9 +56,9 @@ __global__ void __launch_bounds__(kHistThreads, 4)
 #pragma unroll
         for (int u = 0; u < kHistUnroll; ++u) v[u] = ld_stream_v4(in_al + ((c + u * stride) << 4));
 #pragma unroll
-        for (int u = 0; u < kHistUnroll; ++u) hist_chunk(hl, v[u]);
+        for (int u = 0; u < kHistUnroll; ++u) hist_chunk(h, lane4, v[u]);
     }
-    for (; c < end_full; c += stride) hist_chunk(hl, ld_stream_v4(in_al + (c << 4)));
+    for (; c < end_full; c += stride) hist_chunk(h, lane4, ld_stream_v4(in_al + (c << 4)));
 
     // ragged head chunk (0, when lo > 0) and tail chunk (hi >> 4, when hi & 15)
     if (blockIdx.x == 0 && threadIdx.x < 2) {
@@ -63,7 +70,7 @@ __global__ void __launch_bounds__(kHistThreads, 4)
             for (uint64_t b = q << 4; b < (q << 4) + 16; ++b) {
                 if (b < lo || b >= hi) continue;
                 const uint32_t byte = (wv[(b & 15) >> 2] >> (8 * (b & 3))) & 0xffu;
-                atomicAdd(hl + (byte << 5), 1u);
+                hist_add(h, (byte << 7) | lane4);
             }
         }
     }
@@ -88,7 +95,7 @@ __global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const __grid_c
     for (int i = threadIdx.x; i < 256 * 32; i += kHistThreads) h[i] = 0;
     __syncthreads();
     const uint32_t tid = threadIdx.x;
-    uint32_t* hl = h + (tid & 31);
+    const uint32_t lane4 = (tid & 31) << 2;
     uint32_t prev = 0, acc = 0;  // running fold of bin `tid` (tid < 256); the job's sum so far
     const uint64_t nitems = a.nitems_dev ? *a.nitems_dev : a.nitems;
     const uint64_t per = (nitems + gridDim.x - 1) / gridDim.x;
@@ -109,9 +116,9 @@ __global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const __grid_c
 #pragma unroll
             for (int u = 0; u < kHistUnroll; ++u) v[u] = ld_stream_v4(in + ((c + u * kHistThreads) << 4));
 #pragma unroll
-            for (int u = 0; u < kHistUnroll; ++u) hist_chunk(hl, v[u]);
+            for (int u = 0; u < kHistUnroll; ++u) hist_chunk(h, lane4, v[u]);
         }
-        for (; c < c1; c += kHistThreads) hist_chunk(hl, ld_stream_v4(in + (c << 4)));
+        for (; c < c1; c += kHistThreads) hist_chunk(h, lane4, ld_stream_v4(in + (c << 4)));
         // ragged head chunk (a job's first region only) and tail chunk (its last only)
         uint64_t q = ~0ull;
         if (tid == 0 && (lo_v & 15)) q = lo_v >> 4;
@@ -121,7 +128,7 @@ __global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const __grid_c
             const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
             for (uint64_t b = q << 4; b < (q << 4) + 16; ++b) {
                 if (b < lo_v || b >= v1) continue;
-                atomicAdd(hl + (((wv[(b & 15) >> 2] >> (8 * (b & 3))) & 0xffu) << 5), 1u);
+                hist_add(h, (((wv[(b & 15) >> 2] >> (8 * (b & 3))) & 0xffu) << 7) | lane4);
             }
         }
         __syncthreads();
@@ -150,14 +157,10 @@ __global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const __grid_c
 // `hist` must be zeroed by the caller ([count][256]).
 int launch_hist_st(const HistStArgs& a, int ctas_per_sm, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    static int sms = 0, per_sm = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hist_st_kernel, kHistThreads, 0);
-        if (per_sm < 1) per_sm = 1;
-    }
+    static LaunchCache cache;
+    const LaunchFacts f = cache.get(reinterpret_cast<const void*>(hist_st_kernel), kHistThreads, 0);
+    if (f.err != cudaSuccess) return f.err;
+    const int sms = f.sms, per_sm = f.per_sm;
     const int k = (ctas_per_sm > 0 && ctas_per_sm < per_sm) ? ctas_per_sm : per_sm;
     const uint64_t cap = (uint64_t)sms * k;
     const unsigned grid = (unsigned)(a.nitems_dev ? cap : (a.nitems < cap ? (a.nitems ? a.nitems : 1) : cap));
@@ -172,14 +175,10 @@ int launch_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, void* strea
     const uintptr_t addr = reinterpret_cast<uintptr_t>(d_in);
     const uint64_t lo = addr & 15;
     const uint8_t* al = reinterpret_cast<const uint8_t*>(addr - lo);
-    static int sms = 0, per_sm = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hist_kernel, kHistThreads, 0);
-        if (per_sm < 1) per_sm = 1;
-    }
+    static LaunchCache cache;
+    const LaunchFacts f = cache.get(reinterpret_cast<const void*>(hist_kernel), kHistThreads, 0);
+    if (f.err != cudaSuccess) return f.err;
+    const int sms = f.sms, per_sm = f.per_sm;
     const uint64_t chunks = (lo + n + 15) >> 4;
     uint64_t want = (chunks + (uint64_t)kHistThreads * kHistUnroll - 1) / ((uint64_t)kHistThreads * kHistUnroll);
     const uint64_t cap = (uint64_t)sms * per_sm;

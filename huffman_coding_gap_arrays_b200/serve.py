@@ -6,7 +6,9 @@ batched path -- arrive over time.  The loop, running on the host:
 
   * admits arrived requests, oldest first, into the next batch while the
     batch stays under ``max_batch`` requests and the device memory the
-    in-flight batches hold stays under the HBM budget;
+    in-flight batches hold stays under the HBM budget (a batch is admitted on
+    an upper bound of its allocations from the library's own size queries,
+    and then charged the bytes it really allocated);
   * launches each batch as one batched compress and/or one batched
     decompress on its own stream (up to ``max_inflight`` batches at once,
     so requests that arrive while others are on the GPU start as soon as a
@@ -17,9 +19,11 @@ batched path -- arrive over time.  The loop, running on the host:
 Codebooks and decoder tables are built on the device inside each batch and
 never leave it.  Payloads and results stay in HBM (the latency is queueing
 plus GPU service, not network or PCIe time).  The launch shape of each batch
-comes from a ``LearnedTuner`` (its features: the batch's size and the
-traffic's measured byte statistics), from one fixed shape, or -- for
-comparison -- requests run one by one through the plain single-buffer path.
+comes from a ``LearnedTuner`` (its features: the batch's own size and byte
+statistics -- a decompress request's from its codebook and stream size, a
+compress request's from the traffic compressed so far), from one fixed shape,
+or -- for comparison -- requests run one by one through the plain
+single-buffer path.
 """
 from __future__ import annotations
 
@@ -55,6 +59,18 @@ class Request:
         return int(self.data.numel()) if self.kind == "compress" else int(self.stream.entry.n)
 
 
+def entry_features(e) -> np.ndarray:
+    """Byte statistics of one encoded stream from its entry alone: code bits
+    per byte (the code's mean length, within a bit of the entropy), the
+    longest code, and the share of bytes with codes longer than the decoder's
+    11-bit level-1 prefix, as the code itself implies (a code of length l
+    stands for probability 2^-l)."""
+    lens = np.array([e.symbols[k].length for k in range(e.symbol_count)], np.float64)
+    if e.n == 0 or lens.size == 0:
+        return np.zeros(3, np.float32)
+    return np.array([e.bits / e.n, lens.max(), float(np.exp2(-lens[lens > 11]).sum())], np.float32)
+
+
 @dataclass
 class EncodedStream:
     """One buffer's encoded stream in device memory, as the batched path
@@ -63,6 +79,11 @@ class EncodedStream:
     bits: torch.Tensor   # int32 view of u32 words, 16-byte aligned start
     gaps: torch.Tensor
     owner: object = None  # keeps the arenas the views point into alive
+    features: np.ndarray | None = None
+
+    def __post_init__(self):
+        if self.features is None:
+            self.features = entry_features(self.entry)
 
     def to_compressed(self):
         e = self.entry
@@ -71,6 +92,18 @@ class EncodedStream:
         book = codec.Codebook.from_symbols(syms, lens)
         sizes = codec.StreamSizes(int(e.bits), int(e.words), int(e.segments), int(e.gap_words))
         return codec.Compressed(book, int(e.n), sizes, self.bits, self.gaps)
+
+
+ALLOC_GRAIN = 512  # the caching allocator rounds every block up to a multiple of this
+
+
+def _grain(n: int) -> int:
+    return (int(n) + ALLOC_GRAIN - 1) // ALLOC_GRAIN * ALLOC_GRAIN
+
+
+def _q(fn, sizes) -> int:
+    a = np.ascontiguousarray(np.asarray(sizes, np.uint64))
+    return int(fn(len(a), a.ctypes.data_as(C.POINTER(C.c_uint64))))
 
 
 @dataclass
@@ -114,24 +147,65 @@ class Server:
         self.held = 0
         self.peak_held = 0
         self.batches = 0
+        self.mem_waits = 0        # admissions stopped by the HBM budget
+        self.slot_waits = 0       # loop passes with requests ready but every slot busy
+        self.bound_misses = 0     # batches that allocated more than their admission bound
+        # a batch's fixed part per kind: the workspace header, and the allocator's
+        # rounding of each of its tensors (8 for compress, 3 for decompress)
+        L = lib()
+        cfg = LaunchConfig(region_chunks=1).cstruct()
+        self._fixed = {"compress": _grain(L.hgap_batch_compress_workspace_bytes(0, None, C.byref(cfg)))
+                       + 8 * ALLOC_GRAIN,
+                       "decompress": _grain(L.hgap_batch_decompress_workspace_bytes(0, None)) + 4 * ALLOC_GRAIN}
+
+    def reset_counters(self) -> None:
+        """Zeroes the statistics (after a warm-up run)."""
+        self.batches = self.peak_held = self.mem_waits = self.slot_waits = self.bound_misses = 0
 
     # --------------------------------------------------------------- memory
-    @staticmethod
-    def footprint(r: Request) -> int:
-        """Device bytes a request holds while its batch is in flight: the
-        worst-case output arena and workspace for compress, the output and
-        workspace for decompress."""
-        n = r.nbytes
+    def request_bytes(self, r: Request) -> int:
+        """Upper bound of the device bytes a request adds to its batch, from
+        the library's own size queries: for compress, its share of the
+        encoder workspace (whose region count depends on the launch shape:
+        the smallest region is assumed), its worst-case bitstream and gap
+        arena share (16 bits per byte), its entry and pointer slots; for
+        decompress, its output, its share of the decoder workspace, its entry
+        and pointer slots.  Each part rounded as the allocator rounds it,
+        plus the 256-byte alignment of every per-buffer array."""
+        b = getattr(r, "_bytes", None)
+        if b is not None:
+            return b
+        L = lib()
+        n = [r.nbytes]
         if r.kind == "compress":
-            return 2 * n + n // 4 + (1 << 20)
-        return n + n // 64 + (1 << 20)
+            one = LaunchConfig(region_chunks=1).cstruct()
+            ws = int(L.hgap_batch_compress_workspace_bytes(1, np.asarray(n, np.uint64).ctypes.data_as(
+                C.POINTER(C.c_uint64)), C.byref(one))) - int(L.hgap_batch_compress_workspace_bytes(
+                    0, None, C.byref(one)))
+            b = ws + 4 * (_q(L.hgap_batch_bits_capacity, n) + _q(L.hgap_batch_gaps_capacity, n))
+            b += ENTRY_BYTES + 3 * 8 + 6 * 256
+        else:
+            ws = _q(L.hgap_batch_decompress_workspace_bytes, n) - int(L.hgap_batch_decompress_workspace_bytes(0, None))
+            b = _grain(max(r.nbytes, 1)) + ws + ENTRY_BYTES + 8 + 6 * 256
+        r._bytes = int(b)
+        return r._bytes
+
+    def _features(self, reqs) -> np.ndarray:
+        """The batch's own features: log2 of its bytes and the byte-weighted
+        statistics of its requests (a decompress request's from its entry, a
+        compress request's from the traffic compressed so far)."""
+        total = max(1, sum(r.nbytes for r in reqs))
+        acc = np.zeros(3, np.float64)
+        for r in reqs:
+            acc += r.nbytes * (r.stream.features if r.kind == "decompress" else self.traffic)
+        f = np.concatenate([[np.log2(total)], acc / total])
+        # a coarse grid, so the tuner's memo answers most batches without a forward pass
+        return (np.round(f * np.array([8, 2, 1, 50])) / np.array([8, 2, 1, 50])).astype(np.float32)
 
     def _config_for(self, reqs) -> LaunchConfig:
         if self.tuner is None:
             return self.config
-        total = max(1, sum(r.nbytes for r in reqs))
-        f = np.concatenate([[np.log2(total)], self.traffic]).astype(np.float32)
-        return self.tuner.choose(f)
+        return self.tuner.choose(self._features(reqs))
 
     # -------------------------------------------------------------- batches
     def _launch(self, reqs, t0) -> _Batch:
@@ -140,8 +214,9 @@ class Server:
         now = time.perf_counter() - t0
         for r in reqs:
             r.start = now
-        reserved = sum(self.footprint(r) for r in reqs)
-        b = _Batch(reqs, s, torch.cuda.Event(), reserved)
+        bound = self._bound(reqs)
+        before = torch.cuda.memory_allocated(self.device)
+        b = _Batch(reqs, s, torch.cuda.Event(), 0)
         cfg = self._config_for(reqs)
         comp = [r for r in reqs if r.kind == "compress"]
         dec = [r for r in reqs if r.kind == "decompress"]
@@ -151,10 +226,14 @@ class Server:
         # just because the batch landed on another stream than the last one of that size.
         plan = ent = None
         if comp:
-            plan = BatchCodec([r.data.numel() for r in comp], cfg, device=self.device)
+            plan = BatchCodec([r.data.numel() for r in comp], cfg, device=self.device, decompress=False)
             plan.bind([r.data for r in comp])
             ent = torch.empty(plan.entries.numel(), dtype=torch.uint8, pin_memory=True)
         dprep = self._decompress_prepare(dec) if dec else None
+        # the batch is charged what it really holds on the device
+        b.reserved = torch.cuda.memory_allocated(self.device) - before
+        if b.reserved > bound:
+            self.bound_misses += 1
         s.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(s):
             if comp:
@@ -166,6 +245,10 @@ class Server:
                 self._decompress_launch(dec, dprep, cfg, s, b)
         b.event.record(s)
         return b
+
+    def _bound(self, reqs) -> int:
+        kinds = {r.kind for r in reqs}
+        return sum(self.request_bytes(r) for r in reqs) + sum(self._fixed[k] for k in kinds)
 
     def _decompress_prepare(self, reqs):
         """One batched decompress over streams that live anywhere in device
@@ -216,6 +299,9 @@ class Server:
                 bits = b.plan.bits[e.bits_offset:e.bits_offset + e.words]
                 gaps = b.plan.gaps[e.gaps_offset:e.gaps_offset + e.gap_words]
                 r.result = EncodedStream(e, bits, gaps, b.plan) if self.keep_results else int(e.words)
+                # the traffic's byte statistics, for the next batches' features
+                w = min(1.0, r.nbytes / (64 << 20))
+                self.traffic = ((1 - 0.5 * w) * self.traffic + 0.5 * w * entry_features(e)).astype(np.float32)
         if not self.keep_results:
             for r in b.reqs:
                 if r.kind == "decompress":
@@ -257,13 +343,18 @@ class Server:
                 if b.event.query():
                     inflight.remove(b)
                     self._retire(b, time.perf_counter() - t0)
+            if queue and len(inflight) >= self.max_inflight:
+                self.slot_waits += 1
             if queue and len(inflight) < self.max_inflight:
-                take, mem = [], 0
+                take, kinds, mem = [], set(), 0
                 while queue and len(take) < self.max_batch:
-                    f = self.footprint(queue[0])
+                    r = queue[0]
+                    f = self.request_bytes(r) + (0 if r.kind in kinds else self._fixed[r.kind])
                     if self.held + mem + f > self.budget and (take or inflight):
+                        self.mem_waits += 1
                         break  # wait for memory to free up
                     take.append(queue.popleft())
+                    kinds.add(r.kind)
                     mem += f
                 if take:
                     b = self._launch(take, t0)
@@ -296,13 +387,18 @@ class Server:
 
     def _stats(self, reqs, t_end) -> dict:
         lat = np.array([r.done - r.arrival for r in reqs]) * 1e3
+        svc = np.array([r.done - r.start for r in reqs]) * 1e3
         total = sum(r.nbytes for r in reqs)
         return {"requests": len(reqs), "bytes": total, "seconds": round(t_end, 4),
                 "sustained_gbs": round(total / t_end / 1e9, 3),
                 "p50_ms": round(float(np.percentile(lat, 50)), 3),
                 "p99_ms": round(float(np.percentile(lat, 99)), 3),
-                "mean_ms": round(float(lat.mean()), 3), "batches": self.batches,
-                "peak_hbm_gb": round(self.peak_held / 1e9, 3)}
+                "mean_ms": round(float(lat.mean()), 3),
+                "service_p50_ms": round(float(np.percentile(svc, 50)), 3),
+                "service_p99_ms": round(float(np.percentile(svc, 99)), 3), "batches": self.batches,
+                "peak_hbm_gb": round(self.peak_held / 1e9, 3), "budget_gb": round(self.budget / 1e9, 3),
+                "mem_waits": self.mem_waits, "slot_waits": self.slot_waits,
+                "bound_misses": self.bound_misses}
 
 
 def poisson_requests(count: int, rate_gbs: float, pool: torch.Tensor, streams: list, seed: int = 5,

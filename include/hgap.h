@@ -180,6 +180,26 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
  * prepared by hgap_encode_histogram on the same input). */
 hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream);
 
+/* ------------------------------------------------------- bounded-wait hooks
+ * No counterpart in the reference, whose look-back spins never give up
+ * (encoder/src/encoder.cu:239-241, decoder/src/decoder.cu:615-632).  For
+ * testing the bounded waits only: hgap_encode / hgap_decode, except that one
+ * work item, `hold` (encoder: region, decoder: tile, numbered from 0 in stream
+ * order), never publishes its look-back records, and every look-back wait
+ * gives up after `wait_limit_ns` (0: the default of 0.5 s).  The items after
+ * it wait for the withheld record until the limit, the kernel then finishes
+ * with HGAP_ERR_TIMEOUT in the workspace status, and the output is void.
+ * Every write stays inside the output buffers.  hold = UINT64_MAX withholds
+ * nothing (the call is then hgap_encode / hgap_decode with that limit). */
+hgap_status hgap_encode_hold(const void* d_in, uint64_t n, const hgap_codebook* cb, uint32_t* d_bits,
+                             uint64_t words, uint32_t* d_gaps, uint64_t segments, void* d_workspace,
+                             size_t workspace_bytes, hgap_stream_t stream, uint64_t hold,
+                             uint64_t wait_limit_ns);
+hgap_status hgap_decode_hold(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps,
+                             uint64_t segments, const hgap_codebook* cb, uint8_t* d_out, uint64_t n,
+                             void* d_workspace, size_t workspace_bytes, hgap_stream_t stream, uint64_t hold,
+                             uint64_t wait_limit_ns);
+
 /* ------------------------------------------------- decode without allocation
  * No counterpart in the reference: an addition for callers that cannot
  * allocate device memory at all (code inside a framework that owns every
@@ -192,9 +212,11 @@ hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream)
  * rejected with HGAP_ERR_WORKSPACE before anything runs.  The call waits for
  * `stream` and returns the device-side status too.  The first call on each
  * device looks up the array's device address; make it before any stream
- * capture.  All calls share the one array: calls that overlap on the GPU
- * (other streams, other host threads) race and must be serialized by the
- * caller.  Allocates nothing. */
+ * capture.  The address is kept for the life of the process, so a
+ * cudaDeviceReset between calls (which unloads the library's device code and
+ * may move the array) is not supported.  All calls share the one array: calls
+ * that overlap on the GPU (other streams, other host threads) race and must
+ * be serialized by the caller.  Allocates nothing. */
 #define HGAP_NOALLOC_SCRATCH_BYTES (256u * 1024u)
 hgap_status hgap_decode_noalloc(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps,
                                 uint64_t segments, const hgap_codebook* cb, uint8_t* d_out,

@@ -59,11 +59,34 @@ def test_results_are_the_same_alone_and_in_the_mix():
 
 
 def test_hbm_budget_is_respected():
+    """Offered load far above capacity and a budget of a few requests: the
+    admission waits on memory, every batch is charged what it really
+    allocated, which never exceeds its admission bound nor the budget, and
+    every result is still the one the request gets alone."""
     budget = 40 << 20
     server = SV.Server(keep_results=True, hbm_budget=budget, max_batch=64)
     stats, _ = _run(server, 40, 500.0, seed=12, hi=4 << 20)
     assert server.peak_held <= budget, server.peak_held
     assert stats["batches"] > 1
+    assert stats["mem_waits"] > 0
+    assert stats["bound_misses"] == 0
+
+
+def test_request_bound_covers_real_allocations():
+    pool = _pool(nblocks=4)
+    bufs, streams = _streams(pool, k=3)
+    server = SV.Server(keep_results=True)
+    for kind in ("compress", "decompress"):
+        reqs = [SV.Request(i, 0.0, kind, data=b if kind == "compress" else None,
+                           stream=s if kind == "decompress" else None)
+                for i, (b, s) in enumerate(zip(bufs, streams))]
+        torch.cuda.synchronize()
+        b = server._launch(reqs, 0.0)
+        server.held += b.reserved  # as the loop does
+        b.event.synchronize()
+        assert 0 < b.reserved <= server._bound(reqs)
+        server._retire(b, 0.0)
+    assert server.held == 0
 
 
 def test_learned_tuner_policy_and_fixed_shape_agree():
