@@ -318,8 +318,11 @@ def time_reference_kernels(dev, reps: int = 5):
     the same plain-method inputs and with the same timing rules as
     time_plain_kernels: cu_histgram + mergeHistogram; encode() on the device
     (its memsets, cuencoder, cu_get_gaparray) given the reference's own
-    codebook; decoder_l1_l2() on the device (its memsets, gpu_dec_l1_l2).  The
-    reference decoder's output is checked against the input."""
+    codebook; decoder_l1_l2() on the device (its memsets, gpu_dec_l1_l2) on the
+    longest prefix whose stream fills whole 128-segment blocks (its partial
+    last block is unreliable, oracle/ref_gpu.whole_block_prefix; a few KiB
+    short of the input).  The reference decoder's output is checked against
+    the input."""
     import numpy as np
     import torch
     from oracle import oracle as O
@@ -336,7 +339,15 @@ def time_reference_kernels(dev, reps: int = 5):
         _, W, S, G = cb.sizes()
         C = 4 * (W + G)
         t = {k: [] for k in ("hist", "merge", "enc_memset", "cuencoder", "gaparray", "dec_memset", "gpu_dec")}
-        dbufs = None
+        # the reference decoder runs on the longest prefix whose stream fills whole 128-segment
+        # blocks (its partial last block is unreliable: oracle/ref_gpu.whole_block_prefix)
+        m = RG.whole_block_prefix(x, cb)
+        xm = x[:m]
+        bits_m = int(torch.from_numpy(cb.length.astype(np.int64)).to(dev)[xm.long()].sum().item())
+        cbm = RG.with_total_bits(cb, bits_m)
+        _, Wm, Sm, Gm = cbm.sizes()
+        rb, rg, _, _, _ = RG.encode(RG.padded_input(xm, dev), m, cbm)
+        dbufs = RG.DecodeBuffers(rb, rg, m)
         decoded = None
         for r in range(reps + 1):
             flush.zero_()
@@ -344,18 +355,16 @@ def time_reference_kernels(dev, reps: int = 5):
             t["hist"].append(a)
             t["merge"].append(b)
             flush.zero_()
-            bits, gaps, m, e, g = RG.encode(buf, n, cb)
-            t["enc_memset"].append(m)
+            bits, gaps, em, e, g = RG.encode(buf, n, cb)
+            t["enc_memset"].append(em)
             t["cuencoder"].append(e)
             t["gaparray"].append(g)
-            if dbufs is None:
-                dbufs = RG.DecodeBuffers(bits, gaps, n)
             flush.zero_()
-            res = RG.decode(dbufs, S, cb)
+            res = RG.decode(dbufs, Sm, cbm)
             if res is not None:
-                decoded, m, k = res
-                t["dec_memset"].append(m)
-                t["gpu_dec"].append(k)
+                decoded, dm, dk = res
+                t["dec_memset"].append(dm)
+                t["gpu_dec"].append(dk)
             if r == 0:
                 for v in t.values():
                     v.clear()
@@ -368,16 +377,18 @@ def time_reference_kernels(dev, reps: int = 5):
                  "encode_kernels_ms": {"memsets": _median(t["enc_memset"]), "cuencoder": _median(t["cuencoder"]),
                                        "cu_get_gaparray": _median(t["gaparray"])}}
         if t["gpu_dec"]:
-            entry["decode"] = _entry([a + b for a, b in zip(t["dec_memset"], t["gpu_dec"])], n, C + n)
+            Cm = 4 * (Wm + Gm)
+            entry["decode"] = _entry([a + b for a, b in zip(t["dec_memset"], t["gpu_dec"])], m, Cm + m)
             entry["decode_kernels_ms"] = {"memsets": _median(t["dec_memset"]), "gpu_dec_l1_l2": _median(t["gpu_dec"])}
-            entry["decode_round_trip_exact"] = bool(torch.equal(decoded, x))
+            entry["decode_bytes"] = m
+            entry["decode_round_trip_exact"] = bool(torch.equal(decoded, xm))
         else:
             entry["decode"] = None
             entry["decode_skipped"] = "the reference's level-1 table boundary is wrong for this codebook"
         ref_bits = np.asarray(bits.cpu().numpy()).view(np.uint32)
         entry["stream_words"] = int(ref_bits.size)
         out[name] = entry
-        del x, buf, bits, gaps, dbufs, decoded
+        del x, xm, buf, bits, gaps, rb, rg, dbufs, decoded
         torch.cuda.empty_cache()
     return out
 

@@ -27,7 +27,6 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
-#include <mutex>
 
 #include "book.cuh"
 #include "dec_entry.cuh"
@@ -459,38 +458,6 @@ uint64_t worst_tiles(uint32_t count, const uint64_t* sizes) {
 
 inline hgap_status cuda_status(int e) { return e == 0 ? HGAP_OK : HGAP_ERR_CUDA; }
 
-// The decoder classes run concurrently: the caller's stream forks to one side
-// stream per class and joins them again (under stream capture this becomes
-// eight parallel branches of the graph), so one class's persistent grid fills
-// the SMs that another's tail leaves idle.  The side streams and events are
-// created once per device and kept for the life of the process; the mutex
-// makes one call's fork / launches / join sequence atomic with respect to
-// other host threads.
-struct ForkJoin {
-    cudaStream_t side[kClasses];
-    cudaEvent_t fork;
-    cudaEvent_t join[kClasses];
-    cudaError_t err = cudaSuccess;
-};
-
-std::mutex g_fork_mutex;
-
-ForkJoin* fork_join_for_current_device() {
-    static std::once_flag once[kMaxDevices];
-    static ForkJoin fj[kMaxDevices];
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
-    std::call_once(once[dev], [&] {
-        ForkJoin& f = fj[dev];
-        f.err = cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming);
-        for (uint32_t c = 0; c < kClasses && f.err == cudaSuccess; ++c) {
-            f.err = cudaStreamCreateWithFlags(&f.side[c], cudaStreamNonBlocking);
-            if (f.err == cudaSuccess) f.err = cudaEventCreateWithFlags(&f.join[c], cudaEventDisableTiming);
-        }
-    });
-    return fj[dev].err == cudaSuccess ? &fj[dev] : nullptr;
-}
-
 }  // namespace
 }  // namespace hgap
 
@@ -647,10 +614,6 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     DecTable unused;
     std::memset(&unused, 0, sizeof(unused));
     static const uint32_t kMinLen[4] = {4, 3, 2, 1};  // a representative shortest code per stage size
-    ForkJoin* fj = fork_join_for_current_device();
-    if (!fj) return HGAP_ERR_CUDA;
-    std::lock_guard<std::mutex> lock(g_fork_mutex);
-    if (cudaEventRecord(fj->fork, st) != cudaSuccess) return HGAP_ERR_CUDA;
     for (uint32_t c = 0; c < kClasses; ++c) {
         DecArgs a;
         std::memset(&a, 0, sizeof(a));
@@ -664,14 +627,9 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
         a.counter = counters + c;
         a.status = status;
         // batched streams are compressible ones on the whole: always two symbols per lookup where they fit
-        if (cudaStreamWaitEvent(fj->side[c], fj->fork, 0) != cudaSuccess) return HGAP_ERR_CUDA;
-        if (launch_decode(a, unused, kMinLen[c / 2], (c & 1) != 0, true, (int)cfg->dec_ctas_per_sm,
-                          fj->side[c]) != 0)
+        if (launch_decode(a, unused, kMinLen[c / 2], (c & 1) != 0, true, (int)cfg->dec_ctas_per_sm, stream) != 0)
             return HGAP_ERR_CUDA;
-        if (cudaEventRecord(fj->join[c], fj->side[c]) != cudaSuccess) return HGAP_ERR_CUDA;
     }
-    for (uint32_t c = 0; c < kClasses; ++c)
-        if (cudaStreamWaitEvent(st, fj->join[c], 0) != cudaSuccess) return HGAP_ERR_CUDA;
     return HGAP_OK;
 }
 

@@ -5,16 +5,18 @@
 // segment is decoded ONCE (the reference decodes it twice: a counting pass,
 // then a writing pass, decoder.cu:529-569,672-725):
 //   1. a persistent CTA of 256 threads takes the next tile of 512 segments
-//      (256 for books with 1-2 bit codes), stages its bitstream words in
-//      shared memory (padded one word in eight so the threads' windows, 4
-//      words apart, fall in different banks) and every thread decodes its
-//      segments one after the other (interleaving two chains measured slower:
-//      the loop is issue-bound) through a two-level table (level 1 in shared
-//      memory, the rarely used level 2 read from global memory),
-//      parking each segment's symbols in its own shared row sized for the
-//      book's shortest code (a segment holds at most ceil(128 / shortest
-//      length) symbols);
-//   2. block scan of the 512 symbol counts + one bounded decoupled look-back
+//      (256 for books with 1-2 bit codes); every thread takes its segments'
+//      words straight from global memory into registers a tile ahead (one
+//      16-byte load per segment, the next segment's first word from the
+//      neighbouring lane) and decodes them one after the other (interleaving
+//      two chains measured slower: the loop is issue-bound) through a
+//      two-level table (level 1 in shared memory, the rarely used level 2 read
+//      from global memory), one 32-bit phase per word, so the loop tests only
+//      the phase end; each segment's symbols are parked in its own shared row
+//      sized for the book's shortest code (a segment holds at most
+//      ceil(128 / shortest length) symbols);
+//   2. block scan of the symbol counts (both halves of the tile packed in one
+//      warp scan) + one bounded decoupled look-back
 //      with a 64-tile window gives the tile's output offset;
 //   3. the rows are compacted (whole words where the destination is aligned)
 //      into a shared image of the tile's output and written one tile later,
@@ -47,31 +49,21 @@ struct DecCfg {
     static constexpr int kPer = kSegs / kDecThreads;   // segments per thread
     static constexpr int kWarps = kDecThreads / 32;
     static constexpr int kT1 = 1 << kDecPrefix;        // u32 level-1 entries
-    static constexpr int kT2 = kDecT2Cap;              // u16 level-2 entries
-    static constexpr int kWords = 4 * kSegs + 8;       // bitstream words staged per tile
-    static constexpr int kWordsPad = (kWords + kWords / 8 + 8 + 3) & ~3;
-    static constexpr int kWordsPer = (kWords + kDecThreads - 1) / kDecThreads;
     static constexpr int kGapStage = kSegs / 8 + 4;     // gap words of the tile (+1 before)
-    // stage row of one segment (bytes): its symbols, at least 4 bytes of slack for the
-    // unconditional second store of a pair, and an odd number of words so that
+    // stage row of one segment: its symbols (a multi entry's tail store may put two
+    // bytes past the count: 4 spare bytes there), an odd number of words so that
     // the 32 rows a warp writes start in 32 different banks
-    static constexpr int kRow = ((kMaxSym + 4) / 4 | 1) * 4;
+    static constexpr int kRowWords = ((kMaxSym + (dec_multi(R, true) ? 4 : 0) + 3) / 4) | 1;
+    static constexpr int kRow = 4 * kRowWords;
     static constexpr int kStageBytes = kSegs * kRow + 16;
     static constexpr int kCompactBytes = kSegs * kMaxSym + 64;
     static constexpr int kL1Bytes = dec_multi(R, true) ? kT1 : 0;  // multi entries: first-code lengths
     // the level-2 table stays in global memory (or the kernel parameter): codes longer
-    // than the 11-bit prefix are rare, and its 5 KiB buy a fourth CTA per SM for 8 and
-    // 16 stage rows (Zipf(1.2) 0.684 -> 0.592 ms, uniform bytes 0.570 -> 0.481 ms per
-    // 256 MiB); 11 rows stay at three (shared memory), so they keep up to 85 registers
-    // (80 used; 1 % faster than capped at 64), 32 rows at two
-    static constexpr int kMinBlocks = R == 32 ? 2 : (R == 11 ? 3 : 4);
-    static constexpr size_t kSmem = (size_t)(kT1 + kWordsPad + kGapStage) * 4 +
-                                    kStageBytes + kCompactBytes + kL1Bytes;
-    static_assert(kT1 % 4 == 0 && kWordsPad % 4 == 0 && kGapStage % 4 == 0 &&
-                  kStageBytes % 16 == 0, "16-byte aligned areas");
+    // than the 11-bit prefix are rare, and its shared memory buys CTAs per SM
+    static constexpr int kMinBlocks = R == 32 ? 2 : 4;
+    static constexpr size_t kSmem = (size_t)(kT1 + kGapStage) * 4 + kStageBytes + kCompactBytes + kL1Bytes;
+    static_assert(kT1 % 4 == 0 && kGapStage % 4 == 0 && kStageBytes % 16 == 0, "16-byte aligned areas");
 };
-
-__device__ __forceinline__ uint32_t pidx(uint32_t w) { return w + (w >> 3); }
 
 // One codeword from the 32-bit window x at the current position: level-1
 // lookup, level 2 for the rare longer codes.  Returns the widened entry.
@@ -82,6 +74,123 @@ __device__ __forceinline__ uint32_t lookup(const uint32_t* t1, const uint16_t* _
         e = widen_entry(t2[(e & 0xffffu) + ((x << kDecPrefix) >> (32 - wd))]);
     }
     return e;
+}
+
+// The words of one segment in registers: its own four and the next segment's
+// first (a code that starts in the segment may end up to 15 bits into it).
+struct SegWords {
+    uint32_t w0, w1, w2, w3, w4;
+};
+
+// Decodes the codes that start in one 128-bit segment (not the stream's last
+// one), from bit `pos` (its gap offset), as four phases of 32 bits: phase k
+// decodes the codes starting in word k, from the window of words k and k+1,
+// so the loop tests only `pos < 32` -- no word refill, no end test.  Codes of
+// a pair / multi entry all start inside the segment in phases 0-2 (they fit
+// the 11-bit window and phase 2 ends 32 bits before the segment does); in
+// phase 3 that holds while pos <= 21, and the last bits take only the codes
+// that start before bit 32 of the phase.  Returns the end bit of the last
+// code relative to phase 3 (32 + the next gap entry for a valid stream; larger
+// after an invalid code) and advances `out` past the symbols.
+template <bool COMPLETE, bool PAIRS, bool MULTI>
+__device__ __forceinline__ uint32_t decode_segment(const uint32_t* t1, const uint16_t* __restrict__ t2,
+                                                   const uint8_t* l1t, const SegWords& w, uint32_t pos,
+                                                   uint8_t*& out) {
+    constexpr uint32_t kBad = 1u << 16;  // position after an invalid code: every loop ends
+    auto run_fast = [&](uint32_t cw, uint32_t nw, uint32_t stop) {
+        while (pos < stop) {
+            const uint32_t e = lookup(t1, t2, __funnelshift_l(nw, cw, pos));
+            if (!COMPLETE && (e & 0x40000000u)) {
+                pos = kBad;
+                break;
+            }
+            if (MULTI) {
+                out[0] = (uint8_t)e;
+                out[1] = (uint8_t)(e >> 8);
+                out[2] = (uint8_t)(e >> 16);
+                out += 1 + ((e >> 29) & 3u);
+                pos += (e >> 24) & 31u;
+            } else if (PAIRS) {
+                out[0] = (uint8_t)e;
+                out[1] = (uint8_t)(e >> 8);  // a single entry's second byte: overwritten or past the count
+                out += 1 + ((e >> 16) & 1u);
+                pos += e >> 24;
+            } else {
+                *out++ = (uint8_t)e;
+                pos += e >> 24;
+            }
+        }
+    };
+    run_fast(w.w0, w.w1, 32);
+    pos -= 32;
+    run_fast(w.w1, w.w2, 32);
+    pos -= 32;
+    run_fast(w.w2, w.w3, 32);
+    pos -= 32;
+    if (!PAIRS) {
+        run_fast(w.w3, w.w4, 32);
+        return pos;
+    }
+    run_fast(w.w3, w.w4, 32 - kDecPrefix + 1);
+    while (pos < 32) {  // the last bits: only the codes that start before bit 32
+        const uint32_t x = __funnelshift_l(w.w4, w.w3, pos);
+        const uint32_t e = lookup(t1, t2, x);
+        if (!COMPLETE && (e & 0x40000000u)) {
+            pos = kBad;
+            break;
+        }
+        if (MULTI) {
+            const uint32_t tot = (e >> 24) & 31u, more = (e >> 29) & 3u;
+            out[0] = (uint8_t)e;
+            out[1] = (uint8_t)(e >> 8);
+            out[2] = (uint8_t)(e >> 16);
+            if (pos + tot <= 32) {  // every code of the entry ends, so starts, inside
+                out += 1 + more;
+                pos += tot;
+            } else {
+                out += 1;
+                pos += more ? (uint32_t)l1t[x >> (32 - kDecPrefix)] : tot;
+            }
+        } else {
+            const uint32_t tot = e >> 24;
+            const bool pair = (e & 0x10000u) != 0;
+            const uint32_t l1 = pair ? ((e >> 17) & 15u) : tot;
+            const bool two = pair && pos + l1 < 32;
+            out[0] = (uint8_t)e;
+            if (two) out[1] = (uint8_t)(e >> 8);
+            out += two ? 2 : 1;
+            pos += two ? tot : l1;
+        }
+    }
+    return pos;
+}
+
+// The stream's last segment: its codes end at bit `end` (<= 128) and zero
+// padding follows, which may not decode.  One code per step (the first code of
+// any pair or multi entry), the words picked by index.
+template <bool COMPLETE, bool PAIRS, bool MULTI>
+__device__ __forceinline__ uint32_t decode_last_segment(const uint32_t* t1, const uint16_t* __restrict__ t2,
+                                                        const uint8_t* l1t, const SegWords& w, uint32_t pos,
+                                                        uint32_t end, uint8_t* out) {
+    auto word = [&](uint32_t i) { return i == 0 ? w.w0 : i == 1 ? w.w1 : i == 2 ? w.w2 : i == 3 ? w.w3 : w.w4; };
+    uint32_t cnt = 0;
+    while (pos < end) {
+        const uint32_t wi = pos >> 5;
+        const uint32_t x = __funnelshift_l(word(wi + 1), word(wi), pos);
+        const uint32_t e = lookup(t1, t2, x);
+        if (!COMPLETE && (e & 0x40000000u)) break;  // the padding after the final codeword
+        uint32_t len;
+        if (MULTI) {
+            len = ((e >> 29) & 3u) ? (uint32_t)l1t[x >> (32 - kDecPrefix)] : ((e >> 24) & 31u);
+        } else if (PAIRS) {
+            len = (e & 0x10000u) ? ((e >> 17) & 15u) : (e >> 24);
+        } else {
+            len = e >> 24;
+        }
+        out[cnt++] = (uint8_t)e;
+        pos += len;
+    }
+    return cnt;
 }
 
 // A claimed tile and its job, in shared memory.
@@ -104,8 +213,7 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
     using C = DecCfg<R>;
     extern __shared__ __align__(16) uint32_t smem[];
     uint32_t* t1 = smem;
-    uint32_t* sw = smem + C::kT1;
-    uint32_t* sg = sw + C::kWordsPad;                    // gap words: sg[j] = gaps[s0/8 - 1 + j]
+    uint32_t* sg = smem + C::kT1;                         // gap words: sg[j] = gaps[s0/8 - 1 + j]
     uint8_t* stage = reinterpret_cast<uint8_t*>(sg + C::kGapStage);
     uint8_t* compact = stage + C::kStageBytes;
     uint8_t* l1t = compact + C::kCompactBytes;            // multi entries: length of the first code
@@ -149,34 +257,39 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
         }
     };
 
-    // Loads of one tile's bitstream words and gap words into registers
-    // (issued a tile ahead) and their store into shared memory.
-#define HGAP_PREFETCH(S)                                                                      \
-    do {                                                                                      \
-        const DecSlot& ps = slot[S];                                                          \
-        const bool ok = ps.item < s_nitems;                                                   \
-        const uint64_t pw0 = ps.local * (4 * C::kSegs);  /* the tile's first word */          \
-        const uint64_t pg0 = ps.local * (C::kSegs / 8);  /* and first gap word */             \
-        const uint64_t wrem = ok && ps.job.words > pw0 ? ps.job.words - pw0 : 0;              \
-        const uint32_t wavail = wrem < (uint64_t)C::kWords ? (uint32_t)wrem : (uint32_t)C::kWords; \
-        const uint32_t* const wsrc = ps.job.bits + pw0;                                       \
-        _Pragma("unroll") for (int j = 0; j < C::kWordsPer; ++j) {                            \
-            const uint32_t i = tid + j * kDecThreads;                                         \
-            pre[j] = i < wavail ? ld_stream_u32(wsrc + i) : 0u;                               \
-        }                                                                                     \
-        /* sg[j] = gaps[pg0 - 1 + j]: j = 0 exists unless the tile is its job's first */     \
-        const uint64_t grem = ok && ps.job.gap_words + 1 > pg0 ? ps.job.gap_words + 1 - pg0 : 0; \
-        const uint32_t gavail = grem < (uint64_t)C::kGapStage ? (uint32_t)grem : (uint32_t)C::kGapStage; \
-        pre_gap = (tid < gavail && (tid > 0 || pg0 > 0)) ? __ldg(ps.job.gaps + pg0 - 1 + tid) : 0u; \
-    } while (0)
-#define HGAP_COMMIT()                                                                         \
-    do {                                                                                      \
-        _Pragma("unroll") for (int j = 0; j < C::kWordsPer; ++j) {                            \
-            const uint32_t i = tid + j * kDecThreads;                                         \
-            if (i < (uint32_t)C::kWords) sw[pidx(i)] = pre[j];                                \
-        }                                                                                     \
-        if (tid < (uint32_t)C::kGapStage) sg[tid] = pre_gap;                                  \
-    } while (0)
+    // A tile's words go straight from global memory into registers, a tile
+    // ahead: segment col's four words (one 16-byte load where the stream is
+    // 16-byte aligned) and, for lane 31, the first word of the next segment
+    // (the other lanes take it from their neighbour with a shuffle).  Its gap
+    // words are staged in shared memory.
+    uint4 pre_q[C::kPer];
+    uint32_t pre_w4[C::kPer];
+    uint32_t pre_gap = 0;
+    auto prefetch = [&](const DecSlot& ps) {
+        const bool ok = ps.item < s_nitems;
+        const uint64_t s0p = ps.local * C::kSegs;
+        const uint64_t words = ok ? ps.job.words : 0;
+        const uint32_t* const bits = ps.job.bits;
+        const bool al16 = (reinterpret_cast<uintptr_t>(bits) & 15) == 0;
+#pragma unroll
+        for (int k = 0; k < C::kPer; ++k) {
+            const uint64_t w = 4 * (s0p + tid + k * kDecThreads);  // the segment's first word
+            if (al16 && w + 4 <= words) {
+                pre_q[k] = ld_stream_v4(bits + w);
+            } else {
+                pre_q[k].x = w < words ? ld_stream_u32(bits + w) : 0u;
+                pre_q[k].y = w + 1 < words ? ld_stream_u32(bits + w + 1) : 0u;
+                pre_q[k].z = w + 2 < words ? ld_stream_u32(bits + w + 2) : 0u;
+                pre_q[k].w = w + 3 < words ? ld_stream_u32(bits + w + 3) : 0u;
+            }
+            pre_w4[k] = (lane == 31 && w + 4 < words) ? ld_stream_u32(bits + w + 4) : 0u;
+        }
+        // sg[j] = gaps[pg0 - 1 + j]: j = 0 exists unless the tile is its job's first
+        const uint64_t pg0 = ps.local * (C::kSegs / 8);
+        const uint64_t grem = ok && ps.job.gap_words + 1 > pg0 ? ps.job.gap_words + 1 - pg0 : 0;
+        const uint32_t gavail = grem < (uint64_t)C::kGapStage ? (uint32_t)grem : (uint32_t)C::kGapStage;
+        pre_gap = (tid < gavail && (tid > 0 || pg0 > 0)) ? __ldg(ps.job.gaps + pg0 - 1 + tid) : 0u;
+    };
 
     if (!a.jobs) load_tables(tab);
     if (tid == 0) {
@@ -186,17 +299,15 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
     }
     __syncthreads();
     if (a.jobs && slot[0].item < s_nitems) copy_tables(a.tables[slot[0].job_id]);
-    uint32_t pre[C::kWordsPer];
-    uint32_t pre_gap = 0;
-    HGAP_PREFETCH(0);
-    HGAP_COMMIT();
+    prefetch(slot[0]);
+    if (tid < (uint32_t)C::kGapStage) sg[tid] = pre_gap;
     int ti = 0;        // slot of the tile decoded in this iteration
     int prev_s = -1;   // slot of the tile decoded one iteration earlier: its symbols wait in
                        // `compact` (at tile-local offsets) until its output offset is resolved
     uint32_t prev_ct = 0;
 
     for (;;) {
-        __syncthreads();  // (1) words of the tile staged, its tables loaded; `compact` holds prev
+        __syncthreads();  // (1) gap words of the tile staged, its tables loaded; `compact` holds prev
         const DecSlot& T = slot[ti];
         const bool have = T.item < s_nitems;
         if (!have && prev_s < 0) break;
@@ -211,8 +322,7 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
         const uint64_t seg_rem = have ? T.job.segments - s0 : 0;
         const uint32_t nseg = seg_rem < (uint64_t)C::kSegs ? (uint32_t)seg_rem : (uint32_t)C::kSegs;
         const bool last_tile = seg_rem <= (uint64_t)C::kSegs;
-        // (every entry point checks segments == ceil(words / 4); the clamp keeps any
-        // other job inside its staged words)
+        // (every entry point checks segments == ceil(words / 4))
         const uint64_t bits_rem = last_tile && have ? T.job.words * 32 - 128 * s0 : 0;
         const uint32_t end_last = bits_rem < 128ull * nseg ? (uint32_t)bits_rem : 128 * nseg;
         const uint32_t first_gap = s0 ? ~0u : 0u;  // the job's first segment starts at bit 0
@@ -220,123 +330,41 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
         auto gap_at = [&](uint32_t u) -> uint32_t { return (sg[u >> 3] >> (4 * (u & 7))) & 0xfu; };
 
         // ---- 1. decode segments tid (and tid + 256), one after the other -------
-        uint32_t n[2] = {0, 0};
-        if (have) {
+        uint32_t n[C::kPer];
 #pragma unroll
-            for (int k = 0; k < C::kPer; ++k) {
-                const uint32_t col = tid + k * kDecThreads;
-                uint32_t cnt = 0;
-                if (col < nseg) {
-                    const bool last = last_tile && col + 1 == nseg;
-                    uint32_t pos = 128 * col + (gap_at(col + 7) & (col ? ~0u : first_gap));
-                    const uint32_t end = last ? end_last : 128 * col + 128;
-                    bool bad = false;
-                    uint8_t* const row = stage + col * C::kRow;
+        for (int k = 0; k < C::kPer; ++k) {
+            SegWords w;
+            w.w0 = pre_q[k].x;
+            w.w1 = pre_q[k].y;
+            w.w2 = pre_q[k].z;
+            w.w3 = pre_q[k].w;
+            const uint32_t up = __shfl_down_sync(kFull, pre_q[k].x, 1);
+            w.w4 = lane == 31 ? pre_w4[k] : up;
+            const uint32_t col = tid + k * kDecThreads;
+            uint32_t cnt = 0;
+            if (have && col < nseg) {
+                const uint32_t pos = gap_at(col + 7) & (col ? ~0u : first_gap);
+                uint8_t* const row = stage + col * C::kRow;
+                if (last_tile && col + 1 == nseg) {
+                    cnt = decode_last_segment<COMPLETE, PAIRS, MULTI>(t1, t2, l1t, w, pos,
+                                                                      end_last - 128 * col, row);
+                } else {
                     uint8_t* out = row;
-                    // the window's two stream words live in registers; a code moves
-                    // the position by at most 16 bits, so at most one new word per code
-                    uint32_t w = pos >> 5;
-                    uint32_t cw = sw[pidx(w)], nw = sw[pidx(w + 1)];
-                    // every codeword is at least the book's shortest length, so a
-                    // segment yields at most kMaxSym symbols: no count test needed
-                    if (MULTI) {
-                        // while 11 bits remain, every code of a multi entry starts inside
-                        // the segment: all three symbol bytes are stored unconditionally
-                        // (those past the entry's count are overwritten or lie past the
-                        // segment's count)
-                        const int end_multi = (int)end - kDecPrefix;
-                        while ((int)pos <= end_multi) {
-                            const uint32_t e = lookup(t1, t2, __funnelshift_l(nw, cw, pos));
-                            out[0] = (uint8_t)e;
-                            out[1] = (uint8_t)(e >> 8);
-                            out[2] = (uint8_t)(e >> 16);
-                            out += 1 + ((e >> 29) & 3u);
-                            pos += (e >> 24) & 31u;
-                            if ((pos >> 5) != w) {
-                                ++w;
-                                cw = nw;
-                                nw = sw[pidx(w + 1)];
-                            }
-                        }
-                        // the last bits: a whole entry while it ends inside the segment
-                        // (then every code in it starts there), else its first code alone
-                        while (pos < end) {
-                            const uint32_t x = __funnelshift_l(nw, cw, pos);
-                            const uint32_t e = lookup(t1, t2, x);
-                            const uint32_t tot = (e >> 24) & 31u, more = (e >> 29) & 3u;
-                            out[0] = (uint8_t)e;
-                            out[1] = (uint8_t)(e >> 8);
-                            out[2] = (uint8_t)(e >> 16);
-                            if (pos + tot <= end) {
-                                out += 1 + more;
-                                pos += tot;
-                            } else {
-                                out += 1;
-                                pos += more ? (uint32_t)l1t[x >> (32 - kDecPrefix)] : tot;
-                            }
-                            if ((pos >> 5) != w) {
-                                ++w;
-                                cw = nw;
-                                nw = sw[pidx(w + 1)];
-                            }
-                        }
-                    } else if (PAIRS) {
-                        // while 11 bits remain, both codes of a pair entry start inside
-                        // the segment: the second symbol is stored unconditionally (a
-                        // single entry's is overwritten or lies past the count)
-                        const int end_pair = (int)end - kDecPrefix;
-                        while ((int)pos <= end_pair) {
-                            const uint32_t e = lookup(t1, t2, __funnelshift_l(nw, cw, pos));
-                            if (!COMPLETE && (e & 0x40000000u)) break;
-                            out[0] = (uint8_t)e;
-                            out[1] = (uint8_t)(e >> 8);
-                            out += 1 + ((e >> 16) & 1u);
-                            pos += e >> 24;
-                            if ((pos >> 5) != w) {
-                                ++w;
-                                cw = nw;
-                                nw = sw[pidx(w + 1)];
-                            }
-                        }
-                    }
-                    while (!MULTI && pos < end) {
-                        const uint32_t e = lookup(t1, t2, __funnelshift_l(nw, cw, pos));
-                        if (!COMPLETE && (e & 0x40000000u)) {
-                            bad = !last;  // zero padding after the final codeword may not decode
-                            break;
-                        }
-                        if (PAIRS) {
-                            // one or two symbols; the second only if it starts inside the segment
-                            const uint32_t tot = e >> 24;
-                            const bool pair = (e & 0x10000u) != 0;
-                            const uint32_t l1 = pair ? ((e >> 17) & 15u) : tot;
-                            const bool two = pair && pos + l1 < end;
-                            out[0] = (uint8_t)e;
-                            if (two) out[1] = (uint8_t)(e >> 8);
-                            out += two ? 2 : 1;
-                            pos += two ? tot : l1;
-                        } else {
-                            *out++ = (uint8_t)e;
-                            pos += e >> 24;
-                        }
-                        if ((pos >> 5) != w) {
-                            ++w;
-                            cw = nw;
-                            nw = sw[pidx(w + 1)];
-                        }
-                    }
+                    const uint32_t e = decode_segment<COMPLETE, PAIRS, MULTI>(t1, t2, l1t, w, pos, out);
                     cnt = (uint32_t)(out - row);
-                    if (!last && !bad && pos != 128 * col + 128 + gap_at(col + 8)) bad = true;
-                    if (bad) atomicOr(a.status, kDevCorrupt);
+                    if (e != 32 + gap_at(col + 8)) atomicOr(a.status, kDevCorrupt);
                 }
-                n[k] = cnt;
             }
+            n[k] = cnt;
         }
 
-        // ---- 2. scan of the 512 counts (segments 0..255 are k = 0, 256..511 k = 1)
-        const uint32_t i0 = warp_incl_scan(n[0], lane);
-        const uint32_t i1 = warp_incl_scan(n[1], lane);
-        if (lane == 31) warp_tot[warp] = i0 | (i1 << 16);  // a warp's 32 segments: < 2^13 symbols
+        // ---- 2. scan of the counts: both halves of the tile at once, packed in
+        //         16-bit fields (a warp's 32 segments hold < 2^13 symbols)
+        uint32_t packed = 0;
+#pragma unroll
+        for (int k = 0; k < C::kPer; ++k) packed |= n[k] << (16 * k);
+        const uint32_t incl = warp_incl_scan(packed, lane);
+        if (lane == 31) warp_tot[warp] = incl;
         if (tid == 0) {
             if (have) fill_slot(ns, claim);
             else slot[ns].item = ~0ull;
@@ -344,17 +372,18 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
         __syncthreads();  // (2) decode done; next tile known
         const DecSlot& N = slot[ns];
         const bool have_next = N.item < s_nitems;
-        uint32_t wt = lane < (uint32_t)C::kWarps ? warp_tot[lane] : 0u;
-        uint32_t w0 = warp_incl_scan(wt & 0xffffu, lane), w1 = warp_incl_scan(wt >> 16, lane);
-        const uint32_t total0 = __shfl_sync(kFull, w0, C::kWarps - 1);
-        const uint32_t total1 = __shfl_sync(kFull, w1, C::kWarps - 1);
-        const uint32_t before0 = warp ? __shfl_sync(kFull, w0, warp - 1) : 0u;
-        const uint32_t before1 = warp ? __shfl_sync(kFull, w1, warp - 1) : 0u;
-        const uint32_t Ct = total0 + total1;
-        const uint32_t excl[2] = {before0 + i0 - n[0], total0 + before1 + i1 - n[1]};
+        const uint32_t wt = warp_incl_scan(lane < (uint32_t)C::kWarps ? warp_tot[lane] : 0u, lane);
+        const uint32_t totals = __shfl_sync(kFull, wt, C::kWarps - 1);
+        const uint32_t before = warp ? __shfl_sync(kFull, wt, warp - 1) : 0u;
+        const uint32_t total0 = totals & 0xffffu;
+        const uint32_t Ct = total0 + (totals >> 16);
+        const uint32_t ex = before + incl - packed;  // exclusive prefix, both fields
+        uint32_t excl[C::kPer];
+        excl[0] = ex & 0xffffu;
+        if (C::kPer > 1) excl[C::kPer - 1] = total0 + (ex >> 16);
         if (tid == 0 && have && T.job.item0 + T.local + 1 != a.hook.hold_plus1)
             lookback_publish(a.lookback, T.job.item0 + T.local, Ct, T.local == 0);
-        if (have_next) HGAP_PREFETCH(ns);  // in flight while prev is resolved and written
+        if (have_next) prefetch(N);  // in flight while prev is resolved and written
         if (prev_s >= 0 && warp == 0) {
             const DecSlot& Pv = slot[prev_s];
             const uint64_t rec = Pv.job.item0 + Pv.local;
@@ -440,16 +469,14 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
                 if (tl > 2) compact[d + t + 2] = src[t + 2];
             }
         }
-        if (have_next) {  // sw/sg and the tables are no longer read for this tile
+        if (have_next) {  // sg and the tables are no longer read for this tile
             if (a.jobs && N.job_id != s_lut_job) copy_tables(a.tables[N.job_id]);
-            HGAP_COMMIT();
+            if (tid < (uint32_t)C::kGapStage) sg[tid] = pre_gap;
         }
         prev_s = have ? ti : -1;
         prev_ct = Ct;
         ti = ns;
     }
-#undef HGAP_PREFETCH
-#undef HGAP_COMMIT
 }
 
 uint64_t decode_tiles(uint64_t segments, uint32_t min_len) {

@@ -51,10 +51,11 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
 
 // Waits until *p != 0 and returns it.  Bounded: once `limit_ns` of
 // %globaltimer have passed it flags kDevTimeout and returns `fallback`, so the
-// caller finishes its tile and the kernel exits.  If another error is already
-// flagged (a corrupt stream, a missing codeword, ...) it returns `fallback` at
-// once without flagging a timeout: the output is void anyway, and the status
-// word then names the real cause, whatever the timing.
+// caller finishes its tile and the kernel exits; once a timeout is flagged,
+// every other wait gives up at once.  Other errors (a corrupt stream, a
+// missing codeword, ...) never stop a tile from publishing, so they do not end
+// a wait: a timeout is flagged only when a wait really expired, and in a batch
+// the healthy buffers still decode around a corrupt one.
 __device__ __forceinline__ uint64_t wait_nonzero(const uint64_t* p, uint32_t* status, uint64_t fallback,
                                                  uint64_t limit_ns) {
     uint64_t v = ld_relaxed_u64(p);
@@ -64,7 +65,7 @@ __device__ __forceinline__ uint64_t wait_nonzero(const uint64_t* p, uint32_t* st
         v = ld_relaxed_u64(p);
         if (v != 0) return v;
         if ((it & 31) == 0) {
-            if (ld_relaxed_u32(status) != 0) return fallback;
+            if (ld_relaxed_u32(status) & kDevTimeout) return fallback;
             if (global_timer_ns() - t0 > limit_ns) {
                 atomicOr(status, kDevTimeout);
                 return fallback;
@@ -219,7 +220,7 @@ __device__ __forceinline__ uint64_t lookback_resolve(uint64_t* rec, uint64_t til
                 wait_nonzero(rec + i, status, kFlagP, limit_ns);
             }
             __syncwarp();
-            if (ld_relaxed_u32(status) != 0) return excl;  // gave up, or the output is void: the status says so
+            if (ld_relaxed_u32(status) & kDevTimeout) return excl;  // gave up: the status says so
             continue;  // reload the same window
         }
         uint64_t sum = 0;

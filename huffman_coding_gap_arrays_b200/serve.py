@@ -380,7 +380,8 @@ class Server:
                 c = codec.compress(r.data)
                 r.result = c if self.keep_results else int(c.sizes.words)
             else:
-                r.result = codec.decompress(r.stream.to_compressed())
+                y = codec.decompress(r.stream.to_compressed())
+                r.result = y if self.keep_results else None  # the output is released at once
             torch.cuda.synchronize(self.device)
             r.done = time.perf_counter() - t0
         return self._stats(reqs, time.perf_counter() - t0)

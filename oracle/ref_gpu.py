@@ -94,7 +94,15 @@ def encode(buf, n: int, cb: "O.Codebook"):
 class DecodeBuffers:
     """The reference decoder's input (gap array then bitstream, with spare
     words after it) and its oversized output (it writes past n and memsets
-    4 * (gap words + words) bytes, decoder/src/decoder.cu:529,763)."""
+    4 * (gap words + words) bytes, decoder/src/decoder.cu:529,763).
+
+    The output starts zeroed, as the fresh cudaMalloc of decoder_l1_l2 is in
+    practice: the reference clears only 4 * (gap words + words) bytes of it
+    before each launch (decoder.cu:763, less than n for any compressing
+    stream) yet ORs every thread's first and last output word into place
+    (decoder.cu:704,727), so stale bytes beyond its memset would corrupt its
+    output (a reference defect this harness does not trigger; between
+    repetitions that tail holds the previous, identical decode)."""
 
     def __init__(self, bits, gaps, n: int):
         import torch
@@ -104,7 +112,40 @@ class DecodeBuffers:
         self.input[:G].copy_(gaps)
         self.input[G:G + W].copy_(bits)
         self.out_bytes = max(n + 512, 4 * (G + W)) + 4096
-        self.out = torch.empty(self.out_bytes, dtype=torch.uint8, device=bits.device)
+        self.out = torch.zeros(self.out_bytes, dtype=torch.uint8, device=bits.device)
+
+
+def whole_block_prefix(x, cb: "O.Codebook") -> int:
+    """The longest prefix of x (a uint8 device tensor) whose stream under
+    codebook cb fills whole 128-segment blocks of the reference decoder.
+
+    gpu_dec_l1_l2 runs one thread per segment in blocks of 128 and guards
+    the whole body -- warp shuffles and block barriers included -- with
+    `input_ptr < gap_element_num` (decoder/src/decoder.cu:501-520, shuffles
+    and barriers at :571-653), so in a last block that is not full, lanes
+    skip shuffles and barriers the others execute; on B200 its output near
+    the end of such streams is wrong.  On a stream of whole blocks it decodes
+    exactly.  Only the last few thousand bytes are examined: at most 128
+    segments (16 Ki bits) are dropped."""
+    import torch
+    n = x.numel()
+    lens = torch.from_numpy(cb.length.astype(np.int64)).to(x.device)
+    tail = min(n, 1 << 17)
+    tl = lens[x[n - tail:].long()]
+    total = int(cb.total_bits)
+    # bits of the stream when the last k bytes are dropped, k = 0 .. tail
+    drop = torch.cat([torch.zeros(1, dtype=torch.int64, device=x.device), torch.cumsum(tl.flip(0), 0)])
+    bits = total - drop
+    segs = (bits + 127) // 128
+    ok = torch.nonzero((segs % 128 == 0) & (bits > 0)).flatten()
+    if ok.numel() == 0:
+        return 0
+    return n - int(ok[0].item())
+
+
+def with_total_bits(cb: "O.Codebook", bits: int) -> "O.Codebook":
+    """cb for a shorter input: same codes, `bits` stream bits."""
+    return O.Codebook(cb.symbols, cb.lengths, cb.code, cb.length, bits)
 
 
 def decode(bufs: DecodeBuffers, segments: int, cb: "O.Codebook"):

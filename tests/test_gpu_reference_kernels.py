@@ -3,9 +3,10 @@ histogram (cu_histgram + mergeHistogram), its encoder (cuencoder +
 cu_get_gaparray) and its decoder (gpu_dec_l1_l2), built unmodified for
 sm_100a into oracle/_ref/libref_gpu_time.so.  This library's histogram,
 bitstream and gap array must equal the reference kernels' output, and the
-reference decoder must restore the input from either stream.  The reference
-decoder runs only where its own level-1 table boundary is right
-(decoder/src/get_table.cpp:20-27)."""
+reference decoder must restore the input.  The reference decoder runs only
+where its own level-1 table boundary is right (decoder/src/get_table.cpp:20-27)
+and on a stream of whole 128-segment blocks (ref_gpu.whole_block_prefix: its
+last, partial block runs shuffles and barriers with lanes that skipped them)."""
 import numpy as np
 import pytest
 import torch
@@ -44,8 +45,20 @@ def test_reference_kernels_agree_with_ours(cuda, name):
     bits, gaps = H.Encoder(n).encode(x, book, sizes)
     assert torch.equal(bits, bits_r)
     assert torch.equal(gaps, gaps_r)
-    res = RG.decode(RG.DecodeBuffers(bits, gaps, n), sizes.segments, cb)
+    # the reference decoder: on the longest prefix that fills whole blocks, encoded with
+    # the same codebook by both encoders
+    m = RG.whole_block_prefix(x, cb)
+    assert m > 0
+    xp = x[:m]
+    bits_p = int(torch.from_numpy(cb.length.astype(np.int64)).to(x.device)[xp.long()].sum().item())
+    cbp = RG.with_total_bits(cb, bits_p)
+    _, W, S, G = cbp.sizes()
+    assert S % 128 == 0
+    rb, rg, _, _, _ = RG.encode(RG.padded_input(xp, x.device), m, cbp)
+    ob, og = H.Encoder(m).encode(xp, book, H.StreamSizes.from_bits(bits_p))
+    assert torch.equal(ob, rb) and torch.equal(og, rg)
+    res = RG.decode(RG.DecodeBuffers(rb, rg, m), S, cbp)
     if res is None:
         pytest.skip("the reference's level-1 boundary is wrong for this book")
     y, _, _ = res
-    assert torch.equal(y, x)
+    assert torch.equal(y, xp)
