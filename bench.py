@@ -543,7 +543,7 @@ def run_serving(args, pool, learned, fixed_cfg, dev):
         del reqs
         torch.cuda.synchronize()
     if args.serve_overload_requests:
-        gbs, budget = 400.0, 4e9
+        gbs, budget = 400.0, 2e9
         srv = SV.Server(hbm_budget=budget, traffic_features=traffic, device=dev, config=fixed_cfg)
         srv.run(SV.poisson_requests(min(1000, args.serve_overload_requests), gbs, pool, streams, seed=31))
         srv.reset_counters()

@@ -66,12 +66,13 @@ class BatchEntry(C.Structure):
 
 class BatchConfig(C.Structure):
     _fields_ = [("region_chunks", C.c_uint32), ("hist_ctas_per_sm", C.c_uint32),
-                ("enc_ctas_per_sm", C.c_uint32), ("dec_ctas_per_sm", C.c_uint32)]
+                ("enc_ctas_per_sm", C.c_uint32), ("dec_ctas_per_sm", C.c_uint32),
+                ("dec_tile_segs", C.c_uint32)]
 
 
 DEC_T1_ENTRIES = 2048
 DEC_T2_ENTRIES = 2560
-MLP_IN, MLP_HIDDEN, MLP_OUT = 8, 32, 2
+MLP_IN, MLP_HIDDEN, MLP_OUT = 9, 32, 2
 MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_OUT * MLP_HIDDEN + MLP_OUT
 
 

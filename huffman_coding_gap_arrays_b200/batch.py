@@ -37,10 +37,11 @@ class LaunchConfig:
     hist_ctas_per_sm: int = 0   # persistent grids: CTAs per SM (0 = occupancy maximum)
     enc_ctas_per_sm: int = 0
     dec_ctas_per_sm: int = 0
+    dec_tile_segs: int = 0      # decoder tile: 256 or 512 segments (0 = by the book's shortest code)
 
     def cstruct(self) -> BatchConfig:
         return BatchConfig(self.region_chunks, self.hist_ctas_per_sm, self.enc_ctas_per_sm,
-                           self.dec_ctas_per_sm)
+                           self.dec_ctas_per_sm, self.dec_tile_segs)
 
 
 def _u64p(a: np.ndarray):

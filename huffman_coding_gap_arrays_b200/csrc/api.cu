@@ -249,7 +249,7 @@ hgap_status decode_impl(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     // two symbols per lookup pay off once about a third of the lookups yield two
     const bool pairs = hgap::dec_pair_fraction(t) >= 0.3;
     a.hook = hook;
-    return cuda_status(hgap::launch_decode(a, t, min_len, complete, pairs, 0, stream));
+    return cuda_status(hgap::launch_decode(a, t, min_len, complete, pairs, 0, 0, stream));
 }
 
 hgap::LookbackHook hold_hook(uint64_t hold, uint64_t wait_limit_ns) {

@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count
                                                                   const uint32_t* gaps, uint8_t* const* outputs,
                                                                   DecJob* jobs, uint64_t* item0s,
                                                                   uint64_t* class_nitems, uint64_t tiles_cap,
-                                                                  uint32_t* status) {
+                                                                  uint32_t tile_segs, uint32_t* status) {
     __shared__ uint64_t s_warp[32];
     uint64_t carry = 0, ccarry[kClasses] = {};
     for (uint32_t base = 0; base < count; base += kScanThreads) {
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count
         if (j < count) {
             c = cls[j];
             if (c != kNoClass) {  // tiles of the class's decoder
-                const uint64_t segs = dec_tile_segs(dec_stage_rows(c / 2 == 0 ? 4 : 4 - c / 2));
+                const uint64_t segs = dec_tile_segs_for(dec_stage_rows(c / 2 == 0 ? 4 : 4 - c / 2), tile_segs);
                 nt = (entries[j].segments + segs - 1) / segs;
             }
         }
@@ -519,7 +519,7 @@ hgap_status hgap_batch_compress(uint32_t count, const uint8_t* const* d_inputs, 
     if ((reinterpret_cast<uintptr_t>(d_workspace) & 255) || (reinterpret_cast<uintptr_t>(d_bits) & 15) ||
         (reinterpret_cast<uintptr_t>(d_gaps) & 3))
         return HGAP_ERR_INVALID_ARG;
-    const hgap_batch_config dflt = {0, 0, 0, 0};
+    const hgap_batch_config dflt = {0, 0, 0, 0, 0};
     if (!cfg) cfg = &dflt;
     const EncLayout L = enc_layout(count, workspace_bytes);
     if (L.max_regions == 0) return HGAP_ERR_WORKSPACE;
@@ -581,7 +581,7 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     if (count == 0) return HGAP_OK;
     if (!d_entries || !d_bits || !d_gaps || !d_outputs || !d_workspace) return HGAP_ERR_INVALID_ARG;
     if (reinterpret_cast<uintptr_t>(d_workspace) & 255) return HGAP_ERR_INVALID_ARG;
-    const hgap_batch_config dflt = {0, 0, 0, 0};
+    const hgap_batch_config dflt = {0, 0, 0, 0, 0};
     if (!cfg) cfg = &dflt;
     const DecLayout L = dec_layout(count, workspace_bytes);
     if (L.tiles_cap == 0) return HGAP_ERR_WORKSPACE;
@@ -605,7 +605,7 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     bdec_widen_kernel<<<widen_grid(count), kWidenThreads, 0, st>>>(count, tables, cls, wtables);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
     bdec_setup_kernel<<<1, kScanThreads, 0, st>>>(count, d_entries, cls, d_bits, d_gaps, d_outputs, jobs, item0s,
-                                                  class_nitems, L.tiles_cap, status);
+                                                  class_nitems, L.tiles_cap, cfg->dec_tile_segs, status);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
     bdec_map_kernel<<<book_grid(count), 32 * kBookWarps, 0, st>>>(count, jobs, cls, item0s, job_of, L.tiles_cap);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
@@ -627,7 +627,8 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
         a.counter = counters + c;
         a.status = status;
         // batched streams are compressible ones on the whole: always two symbols per lookup where they fit
-        if (launch_decode(a, unused, kMinLen[c / 2], (c & 1) != 0, true, (int)cfg->dec_ctas_per_sm, stream) != 0)
+        if (launch_decode(a, unused, kMinLen[c / 2], (c & 1) != 0, true, (int)cfg->dec_ctas_per_sm,
+                          cfg->dec_tile_segs, stream) != 0)
             return HGAP_ERR_CUDA;
     }
     return HGAP_OK;

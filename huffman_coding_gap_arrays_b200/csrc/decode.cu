@@ -35,17 +35,20 @@
 namespace hgap {
 
 constexpr int kDecThreads = 256;
-// Segments per tile: dec_tile_segs(R) (hgap_internal.h).
+// Segments per tile: dec_tile_segs(R) by default, 256 or 512 by the launch shape
+// (dec_tile_segs_for, hgap_internal.h).
 // Look-back window = 32 * kDecLookK tiles per round trip.  Small is best:
 // the resolve runs between two barriers, and a narrow window costs fewer
 // loads per lane (measured 256 / 128 / 64 / 32 records: 0.731 / 0.679 /
 // 0.674 / 0.683 ms for 256 MiB of the mixed stream).
 constexpr int kDecLookK = 2;
 
-template <int R>  // stage rows of 4 symbols per segment: at most 4R symbols per segment
+// R: stage rows of 4 symbols per segment (at most 4R symbols per segment);
+// SEGS: segments per tile, 256 (one per thread) or 512 (two per thread).
+template <int R, int SEGS>
 struct DecCfg {
     static constexpr int kMaxSym = 4 * R;
-    static constexpr int kSegs = dec_tile_segs(R);
+    static constexpr int kSegs = SEGS;
     static constexpr int kPer = kSegs / kDecThreads;   // segments per thread
     static constexpr int kWarps = kDecThreads / 32;
     static constexpr int kT1 = 1 << kDecPrefix;        // u32 level-1 entries
@@ -60,8 +63,11 @@ struct DecCfg {
     static constexpr int kL1Bytes = dec_multi(R, true) ? kT1 : 0;  // multi entries: first-code lengths
     // the level-2 table stays in global memory (or the kernel parameter): codes longer
     // than the 11-bit prefix are rare, and its shared memory buys CTAs per SM
-    static constexpr int kMinBlocks = R == 32 ? 2 : 4;
     static constexpr size_t kSmem = (size_t)(kT1 + kGapStage) * 4 + kStageBytes + kCompactBytes + kL1Bytes;
+    // CTAs per SM the shared memory allows (227 KiB usable, ~1.5 KiB static and
+    // reserved per CTA), at most 4 (64 registers a thread)
+    static constexpr int kBySmem = (int)((227u * 1024u) / (kSmem + 1536u));
+    static constexpr int kMinBlocks = kBySmem >= 4 ? 4 : (kBySmem < 1 ? 1 : kBySmem);
     static_assert(kT1 % 4 == 0 && kGapStage % 4 == 0 && kStageBytes % 16 == 0, "16-byte aligned areas");
 };
 
@@ -207,10 +213,10 @@ struct DecSlot {
 // PAIRS: level-1 entries carry two symbols where both codes fit in the window
 // (worth it for short-code books; for long codes the extra selects only cost);
 // with a complete book, up to three (multi entries, widen_multi).
-template <int R, bool COMPLETE, bool PAIRS>
-__global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
+template <int R, int SEGS, bool COMPLETE, bool PAIRS>
+__global__ void __launch_bounds__(kDecThreads, DecCfg<R, SEGS>::kMinBlocks)
     decode_kernel(const __grid_constant__ DecArgs a, const __grid_constant__ DecTable tab) {
-    using C = DecCfg<R>;
+    using C = DecCfg<R, SEGS>;
     extern __shared__ __align__(16) uint32_t smem[];
     uint32_t* t1 = smem;
     uint32_t* sg = smem + C::kT1;                         // gap words: sg[j] = gaps[s0/8 - 1 + j]
@@ -479,15 +485,15 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R>::kMinBlocks)
     }
 }
 
-uint64_t decode_tiles(uint64_t segments, uint32_t min_len) {
-    const uint64_t segs = dec_tile_segs(dec_stage_rows(min_len ? min_len : 1));
+uint64_t decode_tiles(uint64_t segments, uint32_t min_len, uint32_t tile_segs) {
+    const uint64_t segs = dec_tile_segs_for(dec_stage_rows(min_len ? min_len : 1), tile_segs);
     return (segments + segs - 1) / segs;
 }
 
-template <int R, bool COMPLETE, bool PAIRS>
+template <int R, int SEGS, bool COMPLETE, bool PAIRS>
 static int launch_decode_r(const DecArgs& a, const DecTable& t, int ctas_per_sm, cudaStream_t st) {
-    using C = DecCfg<R>;
-    auto kern = decode_kernel<R, COMPLETE, PAIRS>;
+    using C = DecCfg<R, SEGS>;
+    auto kern = decode_kernel<R, SEGS, COMPLETE, PAIRS>;
     static LaunchCache cache;  // one per kernel instantiation
     const LaunchFacts f = cache.get(reinterpret_cast<const void*>(kern), kDecThreads, C::kSmem);
     if (f.err != cudaSuccess) return f.err;
@@ -499,25 +505,32 @@ static int launch_decode_r(const DecArgs& a, const DecTable& t, int ctas_per_sm,
     return cudaGetLastError();
 }
 
+template <int R, bool COMPLETE, bool PAIRS>
+static int launch_decode_s(const DecArgs& a, const DecTable& t, int k, uint32_t tile_segs, cudaStream_t st) {
+    if (dec_tile_segs_for(R, tile_segs) == 512) return launch_decode_r<R, (R >= 32 ? 256 : 512), COMPLETE, PAIRS>(a, t, k, st);
+    return launch_decode_r<R, 256, COMPLETE, PAIRS>(a, t, k, st);
+}
+
 template <bool COMPLETE, bool PAIRS>
-static int launch_decode_c(const DecArgs& a, const DecTable& t, uint32_t min_len, int k, cudaStream_t st) {
+static int launch_decode_c(const DecArgs& a, const DecTable& t, uint32_t min_len, int k, uint32_t tile_segs,
+                           cudaStream_t st) {
     switch (dec_stage_rows(min_len)) {
-        case 8: return launch_decode_r<8, COMPLETE, PAIRS>(a, t, k, st);
-        case 11: return launch_decode_r<11, COMPLETE, PAIRS>(a, t, k, st);
-        case 16: return launch_decode_r<16, COMPLETE, PAIRS>(a, t, k, st);
-        default: return launch_decode_r<32, COMPLETE, PAIRS>(a, t, k, st);
+        case 8: return launch_decode_s<8, COMPLETE, PAIRS>(a, t, k, tile_segs, st);
+        case 11: return launch_decode_s<11, COMPLETE, PAIRS>(a, t, k, tile_segs, st);
+        case 16: return launch_decode_s<16, COMPLETE, PAIRS>(a, t, k, tile_segs, st);
+        default: return launch_decode_s<32, COMPLETE, PAIRS>(a, t, k, tile_segs, st);
     }
 }
 
 int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, bool pairs,
-                  int ctas_per_sm, void* stream) {
+                  int ctas_per_sm, uint32_t tile_segs, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (min_len == 0) min_len = 1;
     if (pairs)
-        return complete ? launch_decode_c<true, true>(a, t, min_len, ctas_per_sm, st)
-                        : launch_decode_c<false, true>(a, t, min_len, ctas_per_sm, st);
-    return complete ? launch_decode_c<true, false>(a, t, min_len, ctas_per_sm, st)
-                    : launch_decode_c<false, false>(a, t, min_len, ctas_per_sm, st);
+        return complete ? launch_decode_c<true, true>(a, t, min_len, ctas_per_sm, tile_segs, st)
+                        : launch_decode_c<false, true>(a, t, min_len, ctas_per_sm, tile_segs, st);
+    return complete ? launch_decode_c<true, false>(a, t, min_len, ctas_per_sm, tile_segs, st)
+                    : launch_decode_c<false, false>(a, t, min_len, ctas_per_sm, tile_segs, st);
 }
 
 }  // namespace hgap

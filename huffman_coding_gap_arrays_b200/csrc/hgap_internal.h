@@ -154,6 +154,12 @@ HGAP_HD constexpr int dec_stage_rows(uint32_t min_len) {
 // R = 32, 3 % for R = 16, and 33 % slower for R = 11, where the per-tile
 // work then dominates).
 HGAP_HD constexpr int dec_tile_segs(int R) { return R >= 16 ? 256 : 512; }
+// The same with a launch-shape override of 256 or 512 segments (0: the
+// default).  32 stage rows keep 256: their 512-segment tile would leave one
+// CTA per SM.
+HGAP_HD constexpr int dec_tile_segs_for(int R, uint32_t override_segs) {
+    return R >= 32 ? 256 : (override_segs == 256 || override_segs == 512) ? (int)override_segs : dec_tile_segs(R);
+}
 constexpr int kDecT2Cap = 2560;  // >= the largest complete 16-bit book (see host.cpp)
 constexpr uint16_t kDecInvalid = 0x4000;
 struct DecTable {
@@ -218,14 +224,15 @@ int launch_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, void* strea
 int launch_encode(const EncArgs& a, const EncTable& t, int ctas_per_sm, void* stream);
 int launch_hist_st(const HistStArgs& a, int ctas_per_sm, void* stream);
 int launch_decode(const DecArgs& a, const DecTable& t, uint32_t min_len, bool complete, bool pairs,
-                  int ctas_per_sm, void* stream);
+                  int ctas_per_sm, uint32_t tile_segs, void* stream);
 // Fraction of level-1 entries that decode two symbols (the decoder's pair
 // rate under the code's own distribution, where every 11-bit prefix is
 // equally likely).
 double dec_pair_fraction(const DecTable& t);
 // Tiles of a stream for a book whose shortest code is min_len bits (the
-// decoder's tile size depends on it); min_len = 1 gives the most.
-uint64_t decode_tiles(uint64_t segments, uint32_t min_len);
+// decoder's tile size depends on it, and on a tile-size override, 0: none);
+// min_len = 1 with 256-segment tiles gives the most.
+uint64_t decode_tiles(uint64_t segments, uint32_t min_len, uint32_t tile_segs = 0);
 
 // ------------------------------------------------------------- host helpers -
 void make_enc_table(const hgap_codebook& cb, EncTable* t);

@@ -1,12 +1,12 @@
 // mlp.cu -- the learned launch tuner's network: a small MLP trained and run
 // on the GPU by these kernels (no counterpart in the reference).
 //
-// Network: x[8] -> 32 ReLU -> 32 ReLU -> y[2], fp32.  The input is a batch's
+// Network: x[9] -> 32 ReLU -> 32 ReLU -> y[2], fp32.  The input is a batch's
 // features (log2 size, entropy, longest code, level-2 byte fraction) and a
 // launch shape (encoder region size, histogram / encoder / decoder CTAs per
-// SM), normalised by the host; the outputs are the predicted log times of
+// SM, decoder tile size), normalised by the host; the outputs are the predicted log times of
 // the batched compress and decompress.  Parameters are one flat fp32 array:
-// W1[32][8] b1[32] W2[32][32] b2[32] W3[2][32] b3[2].
+// W1[32][9] b1[32] W2[32][32] b2[32] W3[2][32] b3[2].
 //
 // Kernels: forward (one thread per sample, parameters staged in shared
 // memory); loss + gradient (one thread per sample, the per-sample gradient

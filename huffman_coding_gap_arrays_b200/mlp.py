@@ -4,7 +4,8 @@ compress and decompress times of an input (a batch of buffers, or one buffer)
 move with the launch shape.
 
     X = [log2 size, entropy, longest code, level-2 byte fraction,        (input)
-         log2 region chunks, histogram / encoder / decoder CTAs per SM]   (shape)
+         log2 region chunks, histogram / encoder / decoder CTAs per SM,
+         decoder tile (-1: 256 segments, 0: by the book, 1: 512)]          (shape)
     y = [log compress ms, log decompress ms], each relative to the mean over
         the shapes measured on the same input: only the ranking of shapes for
         one input matters, and the size effect would otherwise swamp it.
@@ -27,22 +28,26 @@ import torch
 from ._lib import MLP_IN, MLP_OUT, MLP_PARAMS, check, lib
 from .batch import LaunchConfig
 from .codec import _stream
-from .tuner import DEC_CTAS, Autotuner, compress_space
+from .tuner import DEC_SPACE, Autotuner, compress_space, with_dec
 
-SHAPES = [(32, 8), (32,), (32, 32), (32,), (2, 32), (2,)]
+SHAPES = [(32, 9), (32,), (32, 32), (32,), (2, 32), (2,)]
 # CTAs per SM that "0" (the occupancy maximum) means for each grid on B200
 MAX_CTAS = {"hist": 4, "enc": 2, "dec": 4}
+
+
+TILE_CODE = {0: 0.0, 256: -1.0, 512: 1.0}
 
 
 def config_vector(cfg: LaunchConfig) -> np.ndarray:
     return np.array([math.log2(max(cfg.region_chunks, 1)),
                      cfg.hist_ctas_per_sm or MAX_CTAS["hist"],
                      cfg.enc_ctas_per_sm or MAX_CTAS["enc"],
-                     cfg.dec_ctas_per_sm or MAX_CTAS["dec"]], np.float32)
+                     cfg.dec_ctas_per_sm or MAX_CTAS["dec"],
+                     TILE_CODE.get(cfg.dec_tile_segs, 0.0)], np.float32)
 
 
 def records_to_xy(records, relative: bool = True):
-    """Autotuner records -> (X n x 8, T n x 2 log-ms targets, NaN = not
+    """Autotuner records -> (X n x 9, T n x 2 log-ms targets, NaN = not
     measured).  With `relative`, each target is taken relative to the mean
     log time of the records with the same features (one tuned input)."""
     X = np.stack([np.concatenate([r.features, config_vector(r.config)]) for r in records]).astype(np.float32)
@@ -138,7 +143,7 @@ class LearnedTuner:
     """Chooses a launch shape per input from the predictions of an ensemble of
     MLPs, with the exhaustive autotuner as the fallback."""
 
-    def __init__(self, mlps=None, space=None, dec_space=DEC_CTAS, max_rmse: float = 0.3,
+    def __init__(self, mlps=None, space=None, dec_space=DEC_SPACE, max_rmse: float = 0.3,
                  margin: float = 0.03, dec_margin: float = 0.05, default: LaunchConfig | None = None):
         self.mlps = list(mlps) if mlps else []
         self.space = list(space) if space is not None else compress_space()
@@ -191,10 +196,10 @@ class LearnedTuner:
         if key in self._memo:
             return self._memo[key]
         d0 = self.default
-        c = self._pick(f, self.space, LaunchConfig(d0.region_chunks, d0.hist_ctas_per_sm, d0.enc_ctas_per_sm,
-                                                   d0.dec_ctas_per_sm), 0, self.margin)
-        dec = [LaunchConfig(c.region_chunks, c.hist_ctas_per_sm, c.enc_ctas_per_sm, d) for d in self.dec_space]
-        dd = LaunchConfig(c.region_chunks, c.hist_ctas_per_sm, c.enc_ctas_per_sm, d0.dec_ctas_per_sm)
+        d0dec = (d0.dec_ctas_per_sm, d0.dec_tile_segs)
+        c = self._pick(f, self.space, with_dec(d0, d0dec), 0, self.margin)
+        dec = [with_dec(c, d) for d in self.dec_space]
+        dd = with_dec(c, d0dec)
         pick = self._pick(f, dec, dd, 1, self.dec_margin)
         self._memo[key] = pick
         return pick
@@ -208,7 +213,8 @@ class LearnedTuner:
             return
         d0 = self.default
         comp = list(self.space)
-        base = LaunchConfig(d0.region_chunks, d0.hist_ctas_per_sm, d0.enc_ctas_per_sm, d0.dec_ctas_per_sm)
+        d0dec = (d0.dec_ctas_per_sm, d0.dec_tile_segs)
+        base = with_dec(d0, d0dec)
         feats = [np.round(np.concatenate([[k], np.asarray(traffic, np.float32)]) * 8) / 8 for k in keys]
         # stage 1: the compress shape for every size at once
         X = np.stack([np.concatenate([f, config_vector(c)]) for f in feats for c in comp + [base]])
@@ -220,9 +226,7 @@ class LearnedTuner:
             i = int(np.argmin(mean))
             picks.append(comp[i] if mean[i] < math.log(1.0 - self.margin) else base)
         # stage 2: the decoder grid for each size's compress shape
-        dec = [[LaunchConfig(c.region_chunks, c.hist_ctas_per_sm, c.enc_ctas_per_sm, d) for d in self.dec_space]
-               + [LaunchConfig(c.region_chunks, c.hist_ctas_per_sm, c.enc_ctas_per_sm, d0.dec_ctas_per_sm)]
-               for c in picks]
+        dec = [[with_dec(c, d) for d in self.dec_space] + [with_dec(c, d0dec)] for c in picks]
         X = np.stack([np.concatenate([f, config_vector(c)]) for f, row in zip(feats, dec) for c in row])
         nd = len(self.dec_space) + 1
         P = np.stack([m.predict(X)[:, 1] for m in self.mlps]).reshape(len(self.mlps), len(feats), nd)

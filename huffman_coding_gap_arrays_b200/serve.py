@@ -94,7 +94,29 @@ class EncodedStream:
         return codec.Compressed(book, int(e.n), sizes, self.bits, self.gaps)
 
 
+# The batch features the tuner sees in serving, on a coarse grid: log2 bytes in
+# 1/8 steps, code bits per byte to a whole bit, the longest code in three bands
+# (11 or less: no level-2 lookups; 12-13; 14 and up) and the level-2 share as
+# none or some.  The server fills the tuner's memo for the whole grid before the
+# clock starts, so no batch waits for a forward pass.
+FEATURE_ENTROPY = tuple(float(e) for e in range(0, 9))
+FEATURE_MAXLEN = (11.0, 13.0, 16.0)
+FEATURE_L2 = (0.0, 0.125)
+
+
+def quantize_features(f) -> np.ndarray:
+    f = np.asarray(f, np.float64)
+    size = np.round(f[0] * 8) / 8
+    ent = float(np.clip(np.round(f[1]), 0, 8))
+    maxlen = 11.0 if f[2] <= 11 else (13.0 if f[2] <= 13 else 16.0)
+    l2 = 0.0 if f[3] < 0.0625 else 0.125
+    return np.array([size, ent, maxlen, l2], np.float32)
+
+
 ALLOC_GRAIN = 512  # the caching allocator rounds every block up to a multiple of this
+# ...and a block of 1 MiB or more may keep an unsplit remainder of up to 1 MiB
+# (the allocator splits a large block only when more than 1 MiB would be left)
+ALLOC_SLACK = ALLOC_GRAIN + (1 << 20)
 
 
 def _grain(n: int) -> int:
@@ -150,17 +172,19 @@ class Server:
         self.mem_waits = 0        # admissions stopped by the HBM budget
         self.slot_waits = 0       # loop passes with requests ready but every slot busy
         self.bound_misses = 0     # batches that allocated more than their admission bound
+        self.tuner_misses = 0     # batches whose launch shape needed a forward pass of the tuner
         # a batch's fixed part per kind: the workspace header, and the allocator's
-        # rounding of each of its tensors (8 for compress, 3 for decompress)
+        # rounding of each of its shared tensors (8 for compress, 3 for decompress)
         L = lib()
         cfg = LaunchConfig(region_chunks=1).cstruct()
-        self._fixed = {"compress": _grain(L.hgap_batch_compress_workspace_bytes(0, None, C.byref(cfg)))
-                       + 8 * ALLOC_GRAIN,
-                       "decompress": _grain(L.hgap_batch_decompress_workspace_bytes(0, None)) + 4 * ALLOC_GRAIN}
+        self._fixed = {"compress": int(L.hgap_batch_compress_workspace_bytes(0, None, C.byref(cfg)))
+                       + 8 * ALLOC_SLACK,
+                       "decompress": int(L.hgap_batch_decompress_workspace_bytes(0, None)) + 3 * ALLOC_SLACK}
 
     def reset_counters(self) -> None:
         """Zeroes the statistics (after a warm-up run)."""
         self.batches = self.peak_held = self.mem_waits = self.slot_waits = self.bound_misses = 0
+        self.tuner_misses = 0
 
     # --------------------------------------------------------------- memory
     def request_bytes(self, r: Request) -> int:
@@ -169,9 +193,10 @@ class Server:
         encoder workspace (whose region count depends on the launch shape:
         the smallest region is assumed), its worst-case bitstream and gap
         arena share (16 bits per byte), its entry and pointer slots; for
-        decompress, its output, its share of the decoder workspace, its entry
-        and pointer slots.  Each part rounded as the allocator rounds it,
-        plus the 256-byte alignment of every per-buffer array."""
+        decompress, its output (a tensor of its own, with the allocator's
+        rounding), its share of the decoder workspace, its entry and pointer
+        slots; plus the 256-byte alignment of every per-buffer array.  The
+        batch's shared tensors add their rounding once (the fixed part)."""
         b = getattr(r, "_bytes", None)
         if b is not None:
             return b
@@ -186,7 +211,7 @@ class Server:
             b += ENTRY_BYTES + 3 * 8 + 6 * 256
         else:
             ws = _q(L.hgap_batch_decompress_workspace_bytes, n) - int(L.hgap_batch_decompress_workspace_bytes(0, None))
-            b = _grain(max(r.nbytes, 1)) + ws + ENTRY_BYTES + 8 + 6 * 256
+            b = max(r.nbytes, 1) + ALLOC_SLACK + ws + ENTRY_BYTES + 8 + 6 * 256
         r._bytes = int(b)
         return r._bytes
 
@@ -198,14 +223,16 @@ class Server:
         acc = np.zeros(3, np.float64)
         for r in reqs:
             acc += r.nbytes * (r.stream.features if r.kind == "decompress" else self.traffic)
-        f = np.concatenate([[np.log2(total)], acc / total])
-        # a coarse grid, so the tuner's memo answers most batches without a forward pass
-        return (np.round(f * np.array([8, 2, 1, 50])) / np.array([8, 2, 1, 50])).astype(np.float32)
+        return quantize_features(np.concatenate([[np.log2(total)], acc / total]))
 
     def _config_for(self, reqs) -> LaunchConfig:
         if self.tuner is None:
             return self.config
-        return self.tuner.choose(self._features(reqs))
+        f = self._features(reqs)
+        memo = getattr(self.tuner, "_memo", None)
+        if memo is not None and tuple((np.round(f * 8) / 8).astype(np.float32).tolist()) not in memo:
+            self.tuner_misses += 1  # a forward pass inside the loop
+        return self.tuner.choose(f)
 
     # -------------------------------------------------------------- batches
     def _launch(self, reqs, t0) -> _Batch:
@@ -314,10 +341,15 @@ class Server:
         latency and throughput statistics."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         if self.policy != "plain" and self.tuner is not None and hasattr(self.tuner, "precompute"):
-            # every batch size the run can form, decided before the clock starts
+            # every batch the run can form, decided before the clock starts: all sizes
+            # from the smallest request to the largest batch, over the feature grid
             sizes = [r.nbytes for r in reqs]
-            self.tuner.precompute(self.traffic, np.log2(max(1, min(sizes))),
-                                  np.log2(max(1, sum(sorted(sizes)[-self.max_batch:]))))
+            lo = np.log2(max(1, min(sizes)))
+            hi = np.log2(max(1, sum(sorted(sizes)[-self.max_batch:])))
+            for e in FEATURE_ENTROPY:
+                for m in FEATURE_MAXLEN:
+                    for l2 in FEATURE_L2:
+                        self.tuner.precompute(np.array([e, m, l2], np.float32), lo, hi)
         # the cyclic garbage collector stays off while the clock runs: a full pass over
         # the run's objects stalled a launch for ~100 ms and every request queued behind it
         gc_on = gc.isenabled()
@@ -399,7 +431,7 @@ class Server:
                 "service_p99_ms": round(float(np.percentile(svc, 99)), 3), "batches": self.batches,
                 "peak_hbm_gb": round(self.peak_held / 1e9, 3), "budget_gb": round(self.budget / 1e9, 3),
                 "mem_waits": self.mem_waits, "slot_waits": self.slot_waits,
-                "bound_misses": self.bound_misses}
+                "bound_misses": self.bound_misses, "tuner_misses": self.tuner_misses}
 
 
 def poisson_requests(count: int, rate_gbs: float, pool: torch.Tensor, streams: list, seed: int = 5,
@@ -435,4 +467,4 @@ def encode_streams(buffers, config: LaunchConfig | None = None) -> list:
                           plan.gaps[e.gaps_offset:e.gaps_offset + e.gap_words], plan) for e in ents]
 
 
-__all__ = ["Server", "Request", "EncodedStream", "poisson_requests", "encode_streams"]
+__all__ = ["Server", "Request", "EncodedStream", "poisson_requests", "encode_streams", "quantize_features"]

@@ -29,6 +29,13 @@ REGIONS = (1, 2, 4, 8, 16, 32)
 HIST_CTAS = (2, 4)
 ENC_CTAS = (1, 2)
 DEC_CTAS = (1, 2, 3, 4)  # decoder CTAs per SM; each stage size is clamped to what fits (4, 3 or 2)
+DEC_TILES = (0, 256, 512)  # decoder tile: by the book's shortest code (0), or 256 / 512 segments for all
+DEC_SPACE = tuple(itertools.product(DEC_CTAS, DEC_TILES))  # (CTAs per SM, tile) pairs
+
+
+def with_dec(cfg: LaunchConfig, dec) -> LaunchConfig:
+    """cfg with the decoder shape `dec` = (CTAs per SM, tile segments)."""
+    return LaunchConfig(cfg.region_chunks, cfg.hist_ctas_per_sm, cfg.enc_ctas_per_sm, dec[0], dec[1])
 
 
 def compress_space():
@@ -91,15 +98,14 @@ class Record:
 @dataclass
 class TuneResult:
     compress: LaunchConfig
-    decompress_ctas: int
+    decompress: tuple  # (CTAs per SM, tile segments)
     compress_ms: float
     decompress_ms: float
     records: list = field(default_factory=list)
 
     @property
     def config(self) -> LaunchConfig:
-        c = self.compress
-        return LaunchConfig(c.region_chunks, c.hist_ctas_per_sm, c.enc_ctas_per_sm, self.decompress_ctas)
+        return with_dec(self.compress, self.decompress)
 
 
 def _time(fn, reps: int, warmup: int) -> float:
@@ -118,7 +124,7 @@ def _time(fn, reps: int, warmup: int) -> float:
 class Autotuner:
     """Exhaustive search of the launch space on the caller's buffers."""
 
-    def __init__(self, reps: int = 3, warmup: int = 1, space=None, dec_space=DEC_CTAS):
+    def __init__(self, reps: int = 3, warmup: int = 1, space=None, dec_space=DEC_SPACE):
         self.reps = reps
         self.warmup = warmup
         self.space = list(space) if space is not None else compress_space()
@@ -127,8 +133,9 @@ class Autotuner:
 
     def tune(self, inputs, outputs, features: np.ndarray | None = None,
              plan: BatchCodec | None = None) -> TuneResult:
-        """Times every compress shape, then every decoder grid on the best
-        compress output; every run is checked by the device status."""
+        """Times every compress shape, then every decoder shape (grid and
+        tile size) on the best compress output; every run is checked by the
+        device status."""
         sizes = [int(t.numel()) for t in inputs]
         if plan is None:
             base = min(c.region_chunks for c in self.space)
@@ -148,16 +155,16 @@ class Autotuner:
         plan.check_compress()
         best_d, best_dms = None, float("inf")
         for d in self.dec_space:
-            plan.config = LaunchConfig(best_c.region_chunks, best_c.hist_ctas_per_sm, best_c.enc_ctas_per_sm, d)
+            plan.config = with_dec(best_c, d)
             ms = _time(plan.decompress, self.reps, self.warmup)
             plan.check_decompress()
             self.records.append(Record(feats, plan.config, float("nan"), ms))
             if ms < best_dms:
                 best_d, best_dms = d, ms
-        plan.config = LaunchConfig(best_c.region_chunks, best_c.hist_ctas_per_sm, best_c.enc_ctas_per_sm, best_d)
+        plan.config = with_dec(best_c, best_d)
         return TuneResult(best_c, best_d, best_ms, best_dms, list(self.records))
 
 
 __all__ = ["Autotuner", "TuneResult", "Record", "compress_space", "buffer_features", "batch_features",
-           "features_from_hist",
-           "REGIONS", "HIST_CTAS", "ENC_CTAS", "DEC_CTAS"]
+           "features_from_hist", "with_dec",
+           "REGIONS", "HIST_CTAS", "ENC_CTAS", "DEC_CTAS", "DEC_TILES", "DEC_SPACE"]

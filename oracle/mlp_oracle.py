@@ -3,15 +3,15 @@ network (huffman_coding_gap_arrays_b200/csrc/mlp.cu), used as the checker of
 its CUDA forward, gradient and Adam kernels.  Nothing in the product imports
 this file.
 
-Network: x[8] -> 32 ReLU -> 32 ReLU -> y[2]; parameters flat as
-W1[32][8] b1[32] W2[32][32] b2[32] W3[2][32] b3[2];
+Network: x[9] -> 32 ReLU -> 32 ReLU -> y[2]; parameters flat as
+W1[32][9] b1[32] W2[32][32] b2[32] W3[2][32] b3[2];
 loss = scale * sum over samples and non-NaN targets of (y - t)^2 / 2.
 """
 from __future__ import annotations
 
 import numpy as np
 
-IN, HID, OUT = 8, 32, 2
+IN, HID, OUT = 9, 32, 2
 SHAPES = [("W1", (HID, IN)), ("b1", (HID,)), ("W2", (HID, HID)), ("b2", (HID,)), ("W3", (OUT, HID)),
           ("b3", (OUT,))]
 PARAMS = sum(int(np.prod(s)) for _, s in SHAPES)

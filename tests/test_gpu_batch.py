@@ -154,7 +154,9 @@ def test_batch_small_buffers_match_oracle():
 
 @pytest.mark.parametrize("cfg", [B.LaunchConfig(region_chunks=1), B.LaunchConfig(region_chunks=32),
                                  B.LaunchConfig(region_chunks=2, hist_ctas_per_sm=1, enc_ctas_per_sm=1,
-                                                dec_ctas_per_sm=1)])
+                                                dec_ctas_per_sm=1),
+                                 B.LaunchConfig(dec_tile_segs=256), B.LaunchConfig(dec_tile_segs=512),
+                                 B.LaunchConfig(dec_ctas_per_sm=2, dec_tile_segs=512)])
 def test_batch_launch_configs_same_output(cfg):
     _roundtrip(SIZES[3:], cfg, seed=7)
 
