@@ -442,7 +442,9 @@ def run_reference(args, rank: int, world: int):
         elif not RG.available():
             ref_gpu = {"unavailable": "oracle/_ref/libref_gpu_time.so not built (reference sources absent)"}
         else:
+            clk = ClockSampler(0)
             ref_gpu = time_reference_kernels(torch.device("cuda", 0))
+            ref_gpu["clocks"] = clk.stop()
             ref_gpu["how"] = ("the reference's own kernels (encoder/src/encoder.cu, decoder/src/decoder.cu, "
                               "unmodified, sm_100a) launched as its histgram()/encode()/decoder_l1_l2() do, "
                               "CUDA events around each, L2 flushed before each repetition, median of 5")
@@ -832,7 +834,9 @@ def run_batch(args, rank, world, dev, pg):
 
     plain_kernels = None
     if rank == 0 and world == 1 and not args.no_kernels:
+        clk = ClockSampler(dev.index or 0)
         plain_kernels = time_plain_kernels(dev)
+        plain_kernels["clocks"] = clk.stop()
         plain_kernels["how"] = ("hgap_histogram / hgap_encode / hgap_decode and the two-call pipeline, CUDA "
                                 "events around each call, L2 flushed before each repetition, median of 5")
 

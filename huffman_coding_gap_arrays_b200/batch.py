@@ -24,10 +24,9 @@ from .codec import Codebook, Compressed, StreamSizes, _stream
 
 ENTRY_BYTES = C.sizeof(BatchEntry)
 # Kernels one batched call launches (csrc/batch.cu): compress = benc_setup, hist_st, book,
-# benc_place, encode; decompress = bdec_book, bdec_widen, bdec_setup, bdec_map and one decoder
-# per class (8).
+# benc_place, encode; decompress = bdec_table, bdec_setup, bdec_map and one decoder per class (8).
 COMPRESS_KERNELS = 5
-DECOMPRESS_KERNELS = 12
+DECOMPRESS_KERNELS = 11
 
 
 @dataclass

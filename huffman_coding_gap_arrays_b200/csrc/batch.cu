@@ -12,11 +12,11 @@
 //   5. encode       the single-buffer encoder kernel over all regions, the
 //                   CTA reloading its code tables when the buffer changes.
 // Decompress:
-//   1. bdec_book    one warp per buffer: checks the book, builds its decoder
-//                   table, and puts the buffer in one of 8 classes (decoder
-//                   stage size by the shortest code x complete book or not);
-//      bdec_widen   one CTA per buffer: the decoder table in the widened form
-//                   the decode kernel keeps in shared memory (DecTableW);
+//   1. bdec_table   one CTA per buffer: checks the book, builds its decoder
+//                   table in shared memory, writes it in the widened form the
+//                   decode kernel keeps in shared memory (DecTableW), and puts
+//                   the buffer in one of 8 classes (decoder stage size by the
+//                   shortest code x complete book or not);
 //   2. bdec_setup   one CTA: tiles per buffer, look-back record numbering,
 //                   and per class the numbering of the class's tiles;
 //   3. bdec_map     tile -> buffer map of each class;
@@ -221,50 +221,130 @@ __device__ __forceinline__ uint32_t class_of(uint32_t min_len, bool complete) {
     return 2 * r + (complete ? 1 : 0);
 }
 
-__global__ void __launch_bounds__(32 * kBookWarps) bdec_book_kernel(uint32_t count,
-                                                                    const hgap_batch_entry* entries,
-                                                                    DecTable* tables, uint8_t* cls,
-                                                                    uint32_t* status) {
-    extern __shared__ __align__(16) unsigned char book_smem[];
-    BookScratch& s = reinterpret_cast<BookScratch*>(book_smem)[threadIdx.x >> 5];
-    const uint32_t lane = threadIdx.x & 31;
-    for (uint32_t j = blockIdx.x * kBookWarps + (threadIdx.x >> 5); j < count; j += gridDim.x * kBookWarps) {
+constexpr int kTableThreads = 256;
+
+// One CTA per buffer: checks the entry, builds its two-level decoder table in
+// shared memory and writes the widened form the decode kernel copies per tile
+// (DecTableW), then classifies the buffer.  The table is the one
+// warp_dec_table builds (book.cuh) -- every level-1 prefix, and every level-2
+// suffix of a prefix whose codes are longer than kDecPrefix bits, takes the
+// symbol whose left-aligned code is the largest not above it; the level-2
+// groups sit in prefix order -- but every thread owns 8 consecutive prefixes
+// and a block scan places the groups, and the widened entries and the level-2
+// groups in use go out with coalesced stores, in one launch.
+__global__ void __launch_bounds__(kTableThreads) bdec_table_kernel(uint32_t count, const hgap_batch_entry* entries,
+                                                                   DecTableW* wtables, uint8_t* cls,
+                                                                   uint32_t* status) {
+    constexpr uint32_t P = kDecPrefix, X = kMaxLen - kDecPrefix;  // 11, 5
+    constexpr uint32_t kT1 = 1u << P, kPer = kT1 / kTableThreads;  // 8 prefixes a thread
+    __shared__ BookScratch s;
+    __shared__ __align__(16) uint16_t s1[kT1];
+    __shared__ __align__(16) uint16_t s2[kDecT2Cap];
+    __shared__ uint32_t s_warp[kTableThreads / 32];
+    __shared__ uint32_t s_kraft;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (uint32_t j = blockIdx.x; j < count; j += gridDim.x) {
         const hgap_batch_entry& e = entries[j];
         const uint32_t n = e.symbol_count;
-        uint32_t c = kNoClass;
         bool bad = n > 256 || e.segments != (e.words + 3) / 4 || e.gap_words != (e.segments + 7) / 8 ||
                    (e.n != 0) != (e.words != 0) || (e.n != 0 && n == 0);
-        if (!bad && n) {
-            const uint32_t kraft = warp_load_symbols(e.symbols, n, s, lane);
-            if (kraft == ~0u) {
-                bad = true;
-            } else if (!warp_dec_table(s, n, tables + j, lane)) {
-                bad = true;
-            } else {
+        if (warp == 0) {
+            const uint32_t kraft = (!bad && n) ? warp_load_symbols(e.symbols, n, s, lane) : 0u;
+            if (lane == 0) s_kraft = kraft;
+        }
+        __syncthreads();
+        const uint32_t kraft = s_kraft;
+        if (n && kraft == ~0u) bad = true;
+        uint32_t c = kNoClass;
+        if (!bad && n) {  // uniform over the CTA
+            // the largest symbol index i >= from with la[i] <= v (la[0] = 0, la ascends)
+            auto advance = [&](uint32_t i, uint32_t v) {
+                while (i + 1 < n && s.la[i + 1] <= v) ++i;
+                return i;
+            };
+            auto search = [&](uint32_t v) {
+                uint32_t lo = 0, hi = n;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (s.la[mid] <= v) lo = mid;
+                    else hi = mid;
+                }
+                return lo;
+            };
+            auto entry = [&](uint32_t i, uint32_t v) -> uint16_t {
+                const uint32_t L = s.clen[i];
+                if (v < s.la[i] || v - s.la[i] >= (1u << (kMaxLen - L))) return kDecInvalid;
+                return (uint16_t)(((L - 1) << 8) | s.sym[i]);
+            };
+            const uint32_t x0 = kPer * tid;
+            // pass 1: the level-1 entries, and the widths of this thread's pointer prefixes
+            uint32_t span = 0, pmask = 0;
+            uint32_t i_first = search(x0 << X), i_last = i_first;
+            const uint32_t i_start = i_first;
+#pragma unroll
+            for (uint32_t k = 0; k < kPer; ++k) {
+                const uint32_t x = x0 + k;
+                const uint32_t v = x << X;
+                i_first = advance(i_first, v);
+                i_last = advance(i_last > i_first ? i_last : i_first, v | ((1u << X) - 1));
+                const uint32_t L = s.clen[i_last];
+                if (L > P && (s.la[i_last] >> X) == x) {
+                    span += 1u << (L - P);
+                    pmask |= 1u << k;
+                } else {
+                    s1[x] = entry(i_first, v);
+                }
+            }
+            // block scan of the spans: the level-2 offset of this thread's first group
+            const uint32_t incl = warp_incl_scan(span, lane);
+            if (lane == 31) s_warp[warp] = incl;
+            __syncthreads();
+            const uint32_t wt = warp_incl_scan(lane < kTableThreads / 32 ? s_warp[lane] : 0u, lane);
+            const uint32_t total = __shfl_sync(kFull, wt, kTableThreads / 32 - 1);
+            uint32_t off = (warp ? __shfl_sync(kFull, wt, warp - 1) : 0u) + incl - span;
+            if (total <= (uint32_t)kDecT2Cap) {  // uniform; larger only for an incomplete book
+                // pass 2: the pointer prefixes and their level-2 groups
+                i_first = i_start;
+                for (uint32_t k = 0; k < kPer; ++k) {
+                    const uint32_t x = x0 + k;
+                    const uint32_t v = x << X;
+                    i_first = advance(i_first, v);
+                    if (!(pmask >> k & 1u)) continue;
+                    i_last = advance(i_first, v | ((1u << X) - 1));
+                    const uint32_t w = s.clen[i_last] - P;
+                    s1[x] = (uint16_t)(0x8000u | (w << 12) | off);
+                    uint32_t i = i_first;
+                    for (uint32_t y = 0; y < (1u << w); ++y) {
+                        const uint32_t vy = v | (y << (X - w));
+                        i = advance(i, vy);
+                        s2[off + y] = entry(i, vy);
+                    }
+                    off += 1u << w;
+                }
+                const uint32_t used = (total + 7) & ~7u;  // whole 16-byte groups, the tail invalid
+                for (uint32_t k = total + tid; k < used; k += kTableThreads) s2[k] = kDecInvalid;
+                __syncthreads();
                 c = class_of(s.clen[0], kraft == (1u << kMaxLen));
+                const bool multi = dec_multi(kStageRows[c >> 1], (c & 1u) != 0);
+                DecTableW& w = wtables[j];
+                for (uint32_t i = tid; i < kT1; i += kTableThreads) {
+                    w.t1[i] = multi ? widen_multi(s1, i) : widen_pair(s1, i);
+                    w.l1[i] = first_len(s1, i);
+                }
+                for (uint32_t i = tid; i < used / 8; i += kTableThreads)
+                    reinterpret_cast<uint4*>(w.t2)[i] = reinterpret_cast<const uint4*>(s2)[i];
+            } else {
+                bad = true;
             }
         }
-        if (lane == 0) {
+        if (tid == 0) {
             if (bad) {
                 atomicOr(status, kDevCorrupt);
                 c = kNoClass;
             }
             cls[j] = (uint8_t)c;
         }
-        __syncwarp();
-    }
-}
-
-constexpr int kWidenThreads = 256;
-
-__global__ void __launch_bounds__(kWidenThreads) bdec_widen_kernel(uint32_t count, const DecTable* tables,
-                                                                   const uint8_t* cls, DecTableW* wtables) {
-    __shared__ __align__(16) uint16_t s1[1 << kDecPrefix];
-    __shared__ uint32_t s_used;
-    for (uint32_t j = blockIdx.x; j < count; j += gridDim.x) {
-        const uint32_t c = cls[j];
-        if (c == kNoClass) continue;  // uniform over the CTA
-        widen_tables(tables[j], dec_multi(kStageRows[c >> 1], (c & 1u) != 0), wtables[j], s1, &s_used);
+        __syncthreads();  // s, s1, s2 are reused for the next buffer
     }
 }
 
@@ -420,12 +500,12 @@ uint64_t worst_regions(uint32_t count, const uint64_t* sizes, const hgap_batch_c
 }
 
 // Decompress workspace: [header 1024: status @0, counters[8] @64, class nitems[8] @128]
-// [jobs] [tables] [widened tables] [classes] [item0s 8 x (count+1)] then the per-tile arrays
+// [jobs] [widened tables] [classes] [item0s 8 x (count+1)] then the per-tile arrays
 // [records | job_of 8 x cap] for as many tiles as the rest holds.
 constexpr size_t kDecPerTile = 8 + 4 * kClasses;
 
 struct DecLayout {
-    size_t jobs, tables, wtables, cls, item0s, records, job_of, fixed;
+    size_t jobs, wtables, cls, item0s, records, job_of, fixed;
     uint64_t tiles_cap;
 };
 
@@ -434,8 +514,6 @@ DecLayout dec_layout(uint32_t count, size_t workspace_bytes) {
     size_t off = 1024;
     L.jobs = off;
     off = align256(off + sizeof(DecJob) * (size_t)count);
-    L.tables = off;
-    off = align256(off + sizeof(DecTable) * (size_t)count);
     L.wtables = off;
     off = align256(off + sizeof(DecTableW) * (size_t)count);
     L.cls = off;
@@ -591,7 +669,6 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     uint32_t* counters = reinterpret_cast<uint32_t*>(ws + 64);
     uint64_t* class_nitems = reinterpret_cast<uint64_t*>(ws + 128);
     DecJob* jobs = reinterpret_cast<DecJob*>(ws + L.jobs);
-    DecTable* tables = reinterpret_cast<DecTable*>(ws + L.tables);
     DecTableW* wtables = reinterpret_cast<DecTableW*>(ws + L.wtables);
     uint8_t* cls = ws + L.cls;
     uint64_t* item0s = reinterpret_cast<uint64_t*>(ws + L.item0s);
@@ -599,10 +676,7 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     uint32_t* job_of = reinterpret_cast<uint32_t*>(ws + L.job_of);
 
     if (cudaMemsetAsync(ws, 0, 1024, st) != cudaSuccess) return HGAP_ERR_CUDA;
-    if (set_book_smem(bdec_book_kernel) != cudaSuccess) return HGAP_ERR_CUDA;
-    bdec_book_kernel<<<book_grid(count), 32 * kBookWarps, kBookSmem, st>>>(count, d_entries, tables, cls, status);
-    if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
-    bdec_widen_kernel<<<widen_grid(count), kWidenThreads, 0, st>>>(count, tables, cls, wtables);
+    bdec_table_kernel<<<widen_grid(count), kTableThreads, 0, st>>>(count, d_entries, wtables, cls, status);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
     bdec_setup_kernel<<<1, kScanThreads, 0, st>>>(count, d_entries, cls, d_bits, d_gaps, d_outputs, jobs, item0s,
                                                   class_nitems, L.tiles_cap, cfg->dec_tile_segs, status);

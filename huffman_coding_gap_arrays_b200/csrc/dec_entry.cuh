@@ -1,7 +1,8 @@
 // dec_entry.cuh -- the decoder's level-1 entries in the u32 form the decode
 // kernel keeps in shared memory, widened from the u16 table (DecTable).  Used
 // by the decode kernel (single path: widened once per CTA) and by the batched
-// path's per-buffer table build (widened once per buffer, copied per tile).
+// path's per-buffer table build (bdec_table_kernel: widened once per buffer,
+// copied per tile).
 #pragma once
 
 #include "hgap_internal.h"
@@ -61,32 +62,6 @@ __device__ __forceinline__ uint32_t widen_multi(const uint16_t* t1src, uint32_t 
 __device__ __forceinline__ uint8_t first_len(const uint16_t* t1src, uint32_t x) {
     const uint32_t e = widen_entry(t1src[x]);
     return (uint8_t)(e & 0xC0000000u ? 0u : e >> 24);
-}
-
-// The widened form of one buffer's tables (DecTableW), for the batched path:
-// one CTA per buffer at a time.  `multi`: the book is complete.
-__device__ inline void widen_tables(const DecTable& t, bool multi, DecTableW& w, uint16_t* s1,
-                                    uint32_t* s_used) {
-    constexpr int kT1 = 1 << kDecPrefix;
-    static_assert(kT1 * 2 / 16 <= 1024, "one 16-byte group per thread");
-    const uint32_t tid = threadIdx.x;
-    for (uint32_t i = tid; i < kT1 * 2 / 16; i += blockDim.x)
-        reinterpret_cast<uint4*>(s1)[i] = reinterpret_cast<const uint4*>(t.t1)[i];
-    if (tid == 0) *s_used = 0;
-    __syncthreads();
-    uint32_t used = 0;
-    for (uint32_t i = tid; i < (uint32_t)kT1; i += blockDim.x) {
-        const uint32_t e = widen_entry(s1[i]);
-        w.t1[i] = multi ? widen_multi(s1, i) : widen_pair(s1, i);
-        w.l1[i] = first_len(s1, i);
-        if (e & 0x80000000u) used = max(used, (e & 0xffffu) + (1u << ((e >> 16) & 7u)));
-    }
-    atomicMax(s_used, used);
-    __syncthreads();
-    const uint32_t groups = (*s_used + 7) / 8;
-    for (uint32_t i = tid; i < groups; i += blockDim.x)
-        reinterpret_cast<uint4*>(w.t2)[i] = reinterpret_cast<const uint4*>(t.t2)[i];
-    __syncthreads();  // s1 and s_used are reused for the next buffer
 }
 
 }  // namespace hgap
