@@ -30,7 +30,8 @@ EXPORTS = [
     "hgap_decode_table_build", "hgap_decode_table_build_device", "hgap_batch_compress_workspace_bytes",
     "hgap_batch_decompress_workspace_bytes", "hgap_batch_bits_capacity", "hgap_batch_gaps_capacity",
     "hgap_batch_compress", "hgap_batch_decompress", "hgap_batch_status", "hgap_mlp_forward",
-    "hgap_mlp_loss_grad", "hgap_mlp_adam", "hgap_encode_hold", "hgap_decode_hold",
+    "hgap_mlp_loss_grad", "hgap_mlp_adam", "hgap_encode_hold", "hgap_decode_hold", "hgap_status_from_word",
+    "hgap_batch_decoder_class",
 ]
 
 
@@ -67,7 +68,7 @@ class BatchEntry(C.Structure):
 class BatchConfig(C.Structure):
     _fields_ = [("region_chunks", C.c_uint32), ("hist_ctas_per_sm", C.c_uint32),
                 ("enc_ctas_per_sm", C.c_uint32), ("dec_ctas_per_sm", C.c_uint32),
-                ("dec_tile_segs", C.c_uint32)]
+                ("dec_tile_segs", C.c_uint32), ("dec_class_mask", C.c_uint32)]
 
 
 DEC_T1_ENTRIES = 2048
@@ -109,6 +110,7 @@ def lib() -> C.CDLL:
     L.hgap_decode_workspace_bytes.restype = C.c_size_t
     L.hgap_decode.argtypes = [vp, u64, vp, u64, C.POINTER(CCodebook), vp, u64, vp, C.c_size_t, vp]
     L.hgap_workspace_status.argtypes = [vp, vp]
+    L.hgap_status_from_word.argtypes = [C.c_uint32]
     L.hgap_encode_hold.argtypes = L.hgap_encode.argtypes + [u64, u64]
     L.hgap_decode_hold.argtypes = L.hgap_decode.argtypes + [u64, u64]
     L.hgap_decode_noalloc.argtypes = [vp, u64, vp, u64, C.POINTER(CCodebook), vp, u64, vp]
@@ -140,6 +142,8 @@ def lib() -> C.CDLL:
     L.hgap_batch_decompress.argtypes = [C.c_uint32, vp, vp, vp, vp, vp, C.c_size_t,
                                         C.POINTER(BatchConfig), vp]
     L.hgap_batch_status.argtypes = [vp, vp]
+    L.hgap_batch_decoder_class.argtypes = [C.POINTER(SymLen), C.c_uint32]
+    L.hgap_batch_decoder_class.restype = C.c_uint32
     L.hgap_mlp_forward.argtypes = [vp, vp, C.c_uint32, vp, vp]
     L.hgap_mlp_loss_grad.argtypes = [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, vp]
     L.hgap_mlp_adam.argtypes = [vp, vp, vp, vp, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float,
@@ -152,7 +156,7 @@ def lib() -> C.CDLL:
                  "hgap_encode", "hgap_encode_histogram", "hgap_encode_prepared", "hgap_encode_part_prepared",
                  "hgap_decode", "hgap_workspace_status", "hgap_container_write",
                  "hgap_container_parse", "hgap_ref_encode", "hgap_ref_decoder_l1_l2",
-                 "hgap_decode_noalloc"):
+                 "hgap_decode_noalloc", "hgap_status_from_word"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -37,10 +37,24 @@ class LaunchConfig:
     enc_ctas_per_sm: int = 0
     dec_ctas_per_sm: int = 0
     dec_tile_segs: int = 0      # decoder tile: 256 or 512 segments (0 = by the book's shortest code)
+    dec_class_mask: int = 0     # decoder classes to launch (0 = all 8; see decoder_class_mask)
 
     def cstruct(self) -> BatchConfig:
         return BatchConfig(self.region_chunks, self.hist_ctas_per_sm, self.enc_ctas_per_sm,
-                           self.dec_ctas_per_sm, self.dec_tile_segs)
+                           self.dec_ctas_per_sm, self.dec_tile_segs, self.dec_class_mask)
+
+
+def decoder_class_mask(entries) -> int:
+    """The decoder classes a batch of entries (BatchEntry, host copies) needs,
+    as hgap_batch_config.dec_class_mask: an empty class then costs no launch."""
+    L = lib()
+    mask = 0
+    for e in entries:
+        if e.symbol_count:
+            c = int(L.hgap_batch_decoder_class(e.symbols, e.symbol_count))
+            if c < 8:
+                mask |= 1 << c
+    return mask
 
 
 def _u64p(a: np.ndarray):
@@ -62,7 +76,7 @@ class BatchCodec:
     """Workspaces, arenas and pointer tables for a fixed list of buffer sizes."""
 
     def __init__(self, sizes, config: LaunchConfig | None = None, device=None,
-                 region_chunks: np.ndarray | None = None, decompress: bool = True):
+                 region_chunks: np.ndarray | None = None, decompress: bool = True, inputs=None, outputs=None):
         self.sizes = np.ascontiguousarray(np.asarray(sizes, dtype=np.uint64))
         self.count = int(self.sizes.size)
         self.config = config or LaunchConfig()
@@ -80,16 +94,26 @@ class BatchCodec:
         self.bits = torch.empty(max(self.bits_capacity, 4), dtype=torch.int32, device=dev)
         self.gaps = torch.empty(max(self.gaps_capacity, 1), dtype=torch.int32, device=dev)
         self.entries = torch.zeros(max(self.count, 1) * ENTRY_BYTES, dtype=torch.uint8, device=dev)
-        self.d_sizes = _upload(self.sizes.view(np.int64), torch.int64, device=dev)
-        self.d_in = torch.zeros(max(self.count, 1), dtype=torch.int64, device=dev)
-        self.d_out = torch.zeros(max(self.count, 1), dtype=torch.int64, device=dev)
+        # sizes, input pointers and output pointers in one device array, uploaded at once
+        k = max(self.count, 1)
+        meta = np.zeros(3 * k, np.int64)
+        meta[:self.count] = self.sizes.view(np.int64)
+        if inputs is not None:
+            self._check(inputs, "inputs")
+            meta[k:k + self.count] = [t.data_ptr() for t in inputs]
+        if outputs is not None:
+            self._check(outputs, "outputs")
+            meta[2 * k:2 * k + self.count] = [t.data_ptr() for t in outputs]
+        self._meta = _upload(meta, torch.int64, device=dev)
+        self.d_sizes, self.d_in, self.d_out = self._meta[:k], self._meta[k:2 * k], self._meta[2 * k:]
         self.d_region = None
         if region_chunks is not None:
             rc = np.asarray(region_chunks, np.uint8)
             if rc.size != self.count:
                 raise ValueError("one region size per buffer")
             self.d_region = _upload(rc, torch.uint8, device=dev)
-        self._inputs = self._outputs = None
+        self._inputs = list(inputs) if inputs is not None else None
+        self._outputs = list(outputs) if outputs is not None else None
 
     # ---------------------------------------------------------------- binding
     def bind(self, inputs=None, outputs=None) -> None:

@@ -303,6 +303,10 @@ hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream)
     if (cudaMemcpyAsync(&flags, d_workspace, sizeof(flags), cudaMemcpyDeviceToHost, st) != cudaSuccess)
         return HGAP_ERR_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return HGAP_ERR_CUDA;
+    return hgap_status_from_word(flags);
+}
+
+hgap_status hgap_status_from_word(uint32_t flags) {
     if (flags & hgap::kDevTimeout) return HGAP_ERR_TIMEOUT;
     if (flags & hgap::kDevNoCode) return HGAP_ERR_NO_CODE;
     if (flags & hgap::kDevCorrupt) return HGAP_ERR_CORRUPT;

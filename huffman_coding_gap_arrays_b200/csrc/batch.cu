@@ -353,7 +353,8 @@ __global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count
                                                                   const uint32_t* gaps, uint8_t* const* outputs,
                                                                   DecJob* jobs, uint64_t* item0s,
                                                                   uint64_t* class_nitems, uint64_t tiles_cap,
-                                                                  uint32_t tile_segs, uint32_t* status) {
+                                                                  uint32_t tile_segs, uint32_t class_mask,
+                                                                  uint32_t* status) {
     __shared__ uint64_t s_warp[32];
     uint64_t carry = 0, ccarry[kClasses] = {};
     for (uint32_t base = 0; base < count; base += kScanThreads) {
@@ -400,6 +401,8 @@ __global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count
     if (threadIdx.x < kClasses) {
         item0s[(uint64_t)threadIdx.x * (count + 1) + count] = ccarry[threadIdx.x];
         class_nitems[threadIdx.x] = fits ? ccarry[threadIdx.x] : 0;
+        // a class the caller left out of the launch holds buffers: they stay undecoded
+        if (class_mask && ccarry[threadIdx.x] && !(class_mask >> threadIdx.x & 1u)) atomicOr(status, kDevPlan);
     }
 }
 
@@ -597,7 +600,7 @@ hgap_status hgap_batch_compress(uint32_t count, const uint8_t* const* d_inputs, 
     if ((reinterpret_cast<uintptr_t>(d_workspace) & 255) || (reinterpret_cast<uintptr_t>(d_bits) & 15) ||
         (reinterpret_cast<uintptr_t>(d_gaps) & 3))
         return HGAP_ERR_INVALID_ARG;
-    const hgap_batch_config dflt = {0, 0, 0, 0, 0};
+    const hgap_batch_config dflt = {0, 0, 0, 0, 0, 0};
     if (!cfg) cfg = &dflt;
     const EncLayout L = enc_layout(count, workspace_bytes);
     if (L.max_regions == 0) return HGAP_ERR_WORKSPACE;
@@ -659,7 +662,7 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     if (count == 0) return HGAP_OK;
     if (!d_entries || !d_bits || !d_gaps || !d_outputs || !d_workspace) return HGAP_ERR_INVALID_ARG;
     if (reinterpret_cast<uintptr_t>(d_workspace) & 255) return HGAP_ERR_INVALID_ARG;
-    const hgap_batch_config dflt = {0, 0, 0, 0, 0};
+    const hgap_batch_config dflt = {0, 0, 0, 0, 0, 0};
     if (!cfg) cfg = &dflt;
     const DecLayout L = dec_layout(count, workspace_bytes);
     if (L.tiles_cap == 0) return HGAP_ERR_WORKSPACE;
@@ -679,7 +682,8 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     bdec_table_kernel<<<widen_grid(count), kTableThreads, 0, st>>>(count, d_entries, wtables, cls, status);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
     bdec_setup_kernel<<<1, kScanThreads, 0, st>>>(count, d_entries, cls, d_bits, d_gaps, d_outputs, jobs, item0s,
-                                                  class_nitems, L.tiles_cap, cfg->dec_tile_segs, status);
+                                                  class_nitems, L.tiles_cap, cfg->dec_tile_segs, cfg->dec_class_mask,
+                                                  status);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
     bdec_map_kernel<<<book_grid(count), 32 * kBookWarps, 0, st>>>(count, jobs, cls, item0s, job_of, L.tiles_cap);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
@@ -689,6 +693,7 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     std::memset(&unused, 0, sizeof(unused));
     static const uint32_t kMinLen[4] = {4, 3, 2, 1};  // a representative shortest code per stage size
     for (uint32_t c = 0; c < kClasses; ++c) {
+        if (cfg->dec_class_mask && !(cfg->dec_class_mask >> c & 1u)) continue;
         DecArgs a;
         std::memset(&a, 0, sizeof(a));
         a.jobs = jobs;
@@ -706,6 +711,21 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
             return HGAP_ERR_CUDA;
     }
     return HGAP_OK;
+}
+
+uint32_t hgap_batch_decoder_class(const hgap_symlen* symbols, uint32_t count) {
+    if (!symbols || count == 0) return kNoClass;
+    uint32_t min_len = kMaxLen;
+    uint64_t kraft = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint32_t L = symbols[i].length;
+        if (L >= 1 && L <= (uint32_t)kMaxLen) {
+            min_len = L < min_len ? L : min_len;
+            kraft += 1ull << (kMaxLen - L);
+        }
+    }
+    const uint32_t r = min_len >= 4 ? 0 : 4 - min_len;
+    return 2 * r + (kraft == (1ull << kMaxLen) ? 1u : 0u);
 }
 
 hgap_status hgap_batch_status(const void* d_workspace, hgap_stream_t stream) {

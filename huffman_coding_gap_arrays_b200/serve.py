@@ -80,10 +80,14 @@ class EncodedStream:
     gaps: torch.Tensor
     owner: object = None  # keeps the arenas the views point into alive
     features: np.ndarray | None = None
+    class_bit: int = 0    # 1 << its decoder class (hgap_batch_decoder_class), 0 when empty
 
     def __post_init__(self):
         if self.features is None:
             self.features = entry_features(self.entry)
+        e = self.entry
+        c = int(lib().hgap_batch_decoder_class(e.symbols, e.symbol_count)) if e.symbol_count else 255
+        self.class_bit = 1 << c if c < 8 else 0
 
     def to_compressed(self):
         e = self.entry
@@ -119,6 +123,18 @@ ALLOC_GRAIN = 512  # the caching allocator rounds every block up to a multiple o
 ALLOC_SLACK = ALLOC_GRAIN + (1 << 20)
 
 
+def _allocated(device: torch.device) -> int:
+    """Bytes the caching allocator has handed out on `device` -- the figure
+    torch.cuda.memory_allocated reports, read from the allocator's nested
+    statistics directly (memory_allocated flattens the whole statistics tree
+    first: ~0.2 ms a call, most of a small batch's host time)."""
+    idx = device.index if device.index is not None else torch.cuda.current_device()
+    try:
+        return int(torch._C._cuda_memoryStats(idx)["allocated_bytes"]["all"]["current"])
+    except (AttributeError, KeyError, TypeError):
+        return int(torch.cuda.memory_allocated(device))
+
+
 def _grain(n: int) -> int:
     return (int(n) + ALLOC_GRAIN - 1) // ALLOC_GRAIN * ALLOC_GRAIN
 
@@ -138,6 +154,7 @@ class _Batch:
     entries_host: torch.Tensor | None = None
     plan: BatchCodec | None = None
     dec_ws: torch.Tensor | None = None
+    status_host: torch.Tensor | None = None  # the workspaces' status words, copied after the launches
 
 
 class Server:
@@ -160,6 +177,9 @@ class Server:
         self.keep_results = keep_results
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.max_inflight)]
         self.free_streams = list(self.streams)  # a new batch only goes to a stream with nothing queued
+        # per stream: pinned room for its batch's two status words (compress, decompress),
+        # copied there behind the launches, so retiring a batch needs no synchronization
+        self.status_host = {s: torch.zeros(2, dtype=torch.int32, pin_memory=True) for s in self.streams}
         if reserve_bytes and self.policy == "batched":
             # one large cached block up front: per-batch allocations of varying size are
             # then carved from it instead of each new size reaching the driver mid-run.
@@ -242,7 +262,7 @@ class Server:
         for r in reqs:
             r.start = now
         bound = self._bound(reqs)
-        before = torch.cuda.memory_allocated(self.device)
+        before = _allocated(self.device)
         b = _Batch(reqs, s, torch.cuda.Event(), 0)
         cfg = self._config_for(reqs)
         comp = [r for r in reqs if r.kind == "compress"]
@@ -253,23 +273,27 @@ class Server:
         # just because the batch landed on another stream than the last one of that size.
         plan = ent = None
         if comp:
-            plan = BatchCodec([r.data.numel() for r in comp], cfg, device=self.device, decompress=False)
-            plan.bind([r.data for r in comp])
+            plan = BatchCodec([r.data.numel() for r in comp], cfg, device=self.device, decompress=False,
+                              inputs=[r.data for r in comp])
             ent = torch.empty(plan.entries.numel(), dtype=torch.uint8, pin_memory=True)
         dprep = self._decompress_prepare(dec) if dec else None
         # the batch is charged what it really holds on the device
-        b.reserved = torch.cuda.memory_allocated(self.device) - before
+        b.reserved = _allocated(self.device) - before
         if b.reserved > bound:
             self.bound_misses += 1
         s.wait_stream(torch.cuda.current_stream(self.device))
+        b.status_host = self.status_host[s]
+        b.status_host.zero_()
         with torch.cuda.stream(s):
             if comp:
                 plan.compress(stream=s)
                 ent.copy_(plan.entries, non_blocking=True)
+                b.status_host[0:1].copy_(plan.enc_ws.view(torch.int32)[0:1], non_blocking=True)
                 b.plan, b.entries_host = plan, ent
                 b.keep.append((comp, plan, ent))
             if dec:
                 self._decompress_launch(dec, dprep, cfg, s, b)
+                b.status_host[1:2].copy_(b.dec_ws.view(torch.int32)[0:1], non_blocking=True)
         b.event.record(s)
         return b
 
@@ -290,16 +314,24 @@ class Server:
             C.memmove(C.byref(arr[i]), C.byref(r.stream.entry), ENTRY_BYTES)
             arr[i].bits_offset = (r.stream.bits.data_ptr() - base_b) // 4
             arr[i].gaps_offset = (r.stream.gaps.data_ptr() - base_g) // 4
-        d_ent = _upload(np.frombuffer(bytes(arr), np.uint8), torch.uint8, device=self.device)
-        d_out = _upload([o.data_ptr() for o in outs], torch.int64, device=self.device)
+        # the entries (576 bytes each) and the output pointers after them, in one upload
+        host = np.empty(count * ENTRY_BYTES + 8 * count, np.uint8)
+        host[:count * ENTRY_BYTES] = np.frombuffer(bytes(arr), np.uint8)
+        host[count * ENTRY_BYTES:].view(np.int64)[:] = [o.data_ptr() for o in outs]
+        meta = _upload(host, torch.uint8, device=self.device)
+        d_ent, d_out = meta[:count * ENTRY_BYTES], meta[count * ENTRY_BYTES:]
         sizes = np.array([r.nbytes for r in reqs], np.uint64)
         nbytes = lib().hgap_batch_decompress_workspace_bytes(count, sizes.ctypes.data_as(C.POINTER(C.c_uint64)))
         ws = torch.empty((nbytes + 7) // 8, dtype=torch.int64, device=self.device)
-        return outs, base_b, base_g, d_ent, d_out, ws
+        mask = 0
+        for r in reqs:
+            mask |= r.stream.class_bit
+        return outs, base_b, base_g, d_ent, d_out, ws, mask
 
     def _decompress_launch(self, reqs, prep, cfg, s, b) -> None:
-        outs, base_b, base_g, d_ent, d_out, ws = prep
+        outs, base_b, base_g, d_ent, d_out, ws, mask = prep
         c = cfg.cstruct()
+        c.dec_class_mask = mask  # the requests' books are known here: empty classes cost no launch
         check(lib().hgap_batch_decompress(len(reqs), d_ent.data_ptr(), base_b, base_g, d_out.data_ptr(),
                                           ws.data_ptr(), ws.numel() * 8, C.byref(c), _stream(s)),
               "hgap_batch_decompress")
@@ -309,11 +341,12 @@ class Server:
         b.dec_ws = ws
 
     def _retire(self, b: _Batch, now: float) -> None:
-        # device status of the batch's launches (the event has fired: no wait)
+        # device status of the batch's launches, copied to pinned memory before its event
+        words = b.status_host.tolist()
         if b.plan is not None:
-            check(lib().hgap_batch_status(b.plan.enc_ws.data_ptr(), _stream(b.stream)), "served compress")
+            check(lib().hgap_status_from_word(words[0] & 0xffffffff), "served compress")
         if b.dec_ws is not None:
-            check(lib().hgap_batch_status(b.dec_ws.data_ptr(), _stream(b.stream)), "served decompress")
+            check(lib().hgap_status_from_word(words[1] & 0xffffffff), "served decompress")
         for r in b.reqs:
             r.done = now
         self.free_streams.append(b.stream)

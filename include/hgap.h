@@ -180,6 +180,11 @@ hgap_status hgap_decode(const uint32_t* d_bits, uint64_t words, const uint32_t* 
  * prepared by hgap_encode_histogram on the same input). */
 hgap_status hgap_workspace_status(const void* d_workspace, hgap_stream_t stream);
 
+/* The same status from the workspace's first 32-bit word, already copied to
+ * the host by the caller (e.g. an asynchronous copy into pinned memory
+ * ordered after the launch): no synchronization, no device access. */
+hgap_status hgap_status_from_word(uint32_t word);
+
 /* ------------------------------------------------------- bounded-wait hooks
  * No counterpart in the reference, whose look-back spins never give up
  * (encoder/src/encoder.cu:239-241, decoder/src/decoder.cu:615-632).  For
@@ -277,7 +282,18 @@ typedef struct hgap_batch_config {
     uint32_t dec_tile_segs;    /* decoder tile, 256 or 512 segments (0 = by the book's shortest
                                   code: 512 from 3 bits up, 256 below); books with a 1-bit code
                                   always take 256 */
+    uint32_t dec_class_mask;   /* decoder classes hgap_batch_decompress launches: bit k as
+                                  hgap_batch_decoder_class numbers them; 0 = all 8.  For callers
+                                  that know their books on the host: an empty class then costs
+                                  no launch.  A buffer whose class is left out is not decoded
+                                  and the call's status is HGAP_ERR_INVALID_ARG. */
 } hgap_batch_config;
+
+/* The decoder class of a buffer from its container-order symbol list (as in
+ * hgap_batch_entry): 2 * s + c, where s = 0, 1, 2, 3 for a shortest code of
+ * 4 bits or more, 3, 2 and 1 bits, and c = 1 for a complete book (Kraft sum
+ * 1); 255 for an empty list.  The class picks the decoder's stage size. */
+uint32_t hgap_batch_decoder_class(const hgap_symlen* symbols, uint32_t count);
 
 /* Worst-case sizes from the uncompressed sizes (host array). */
 size_t hgap_batch_compress_workspace_bytes(uint32_t count, const uint64_t* sizes,

@@ -160,3 +160,36 @@ def test_batch_host_queries():
     # worst case 16 bits per byte, each bitstream rounded up to 16 bytes
     assert L.hgap_batch_bits_capacity(sizes.size, p) == sum(((int(n) * 16 + 31) // 32 + 3) & ~3 for n in sizes)
     assert L.hgap_batch_gaps_capacity(sizes.size, p) == sum(((int(n) * 16 + 127) // 128 + 7) // 8 for n in sizes)
+
+
+def test_status_from_word():
+    """A device status word read on the host maps to the status
+    hgap_workspace_status returns: timeout above no-code above corrupt above
+    size above plan (no GPU needed)."""
+    L = _lib.lib()
+    f = L.hgap_status_from_word
+    assert f(0) == 0
+    assert f(1) == 3 and f(2) == 4 and f(4) == 7 and f(8) == 5 and f(16) == 1
+    assert f(2 | 8) == 4 and f(1 | 2 | 4 | 8) == 3 and f(4 | 8) == 7 and f(8 | 16) == 5
+    assert f(1 << 20) == 0  # bits no kernel sets
+
+
+def test_batch_decoder_class():
+    """Decoder class from a symbol list on the host: 2 * stage + complete."""
+    from huffman_coding_gap_arrays_b200._lib import SymLen
+    L = _lib.lib()
+
+    def cls(lengths):
+        arr = (SymLen * max(len(lengths), 1))()
+        for i, n in enumerate(lengths):
+            arr[i].symbol, arr[i].length = i, n
+        return L.hgap_batch_decoder_class(arr, len(lengths))
+
+    assert cls([]) == 255
+    assert cls([1, 1]) == 7            # complete, shortest code 1 bit
+    assert cls([1]) == 6               # one symbol: Kraft sum 1/2
+    assert cls([2, 2, 2, 2]) == 5
+    assert cls([3, 3, 3, 3]) == 2      # incomplete (Kraft 1/2), 3 bits
+    assert cls([4] * 16) == 1
+    assert cls([8] * 256) == 1
+    assert cls([5] * 8) == 0

@@ -240,6 +240,42 @@ def test_batch_corrupt_entry_is_reported():
     assert torch.equal(outs[0], bufs[0])  # the healthy buffer still decodes
 
 
+def test_batch_class_mask_launches_only_named_classes():
+    """dec_class_mask from the host copies of the entries decodes exactly; a
+    mask that leaves out a class in use is reported (HGAP_ERR_INVALID_ARG) and
+    the buffers of the classes it names still decode."""
+    sizes = [70000, 50000, 30000, 90000, 4096, 0]
+    bufs = _make_buffers(sizes, 61)
+    # a 1-bit shortest code (class 6/7) beside the mixed generator's books
+    bufs[2] = torch.from_numpy(np.where(np.random.default_rng(1).random(30000) < 0.8, 7, 9)
+                               .astype(np.uint8)).cuda()
+    outs = [torch.full((max(n, 1),), 0xA5, dtype=torch.uint8, device="cuda") for n in sizes]
+    plan = B.BatchCodec(sizes)
+    plan.bind(bufs, outs)
+    plan.compress()
+    plan.check_compress()
+    ents = plan.entries_host()
+    mask = B.decoder_class_mask(ents)
+    assert mask >> 6 & 3  # the two-symbol buffer's class
+    plan.config = B.LaunchConfig(dec_class_mask=mask)
+    plan.decompress()
+    plan.check_decompress()
+    for x, o, n in zip(bufs, outs, sizes):
+        assert torch.equal(o[:n], x)
+    c2 = 1 << (mask.bit_length() - 1)  # leave out the highest class in use
+    for o in outs:
+        o.fill_(0xA5)
+    plan.config = B.LaunchConfig(dec_class_mask=mask & ~c2)
+    plan.decompress()
+    with pytest.raises(HgapError) as ei:
+        plan.check_decompress()
+    assert ei.value.status == 1  # HGAP_ERR_INVALID_ARG
+    lib = B.lib()
+    for x, o, n, e in zip(bufs, outs, sizes, ents):
+        if n and not (1 << lib.hgap_batch_decoder_class(e.symbols, e.symbol_count)) & c2:
+            assert torch.equal(o[:n], x)
+
+
 def test_batch_bf16_planes():
     exp, sm = WL.bf16_planes(1 << 20, seed=3)
     sizes = [exp.numel(), sm.numel()]
