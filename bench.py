@@ -475,8 +475,11 @@ def train_learned_tuner(dev):
     shapes = [(64, 64 << 10), (256, 256 << 10), (512, 1 << 20), (128, 4 << 20), (1024, 4 << 20),
               (2048, 1 << 20), (32, 16 << 20), (384, 2 << 20), (1536, 512 << 10), (768, 4 << 20),
               (96, 8 << 20), (2048, 4 << 20), (128, 128 << 10), (1024, 2 << 20), (3000, 4 << 20),
-              (48, 32 << 20), (640, 1 << 20), (2600, 2 << 20), (200, 16 << 20), (4096, 4 << 20)]
-    hold = [(200, 2 << 20), (1200, 4 << 20)]
+              (48, 32 << 20), (640, 1 << 20), (2600, 2 << 20), (200, 16 << 20), (4096, 4 << 20),
+              # the few-request batches of serving (64 KiB .. 64 MiB requests)
+              (1, 64 << 20), (2, 64 << 20), (3, 64 << 20), (1, 8 << 20), (2, 16 << 20), (4, 64 << 20),
+              (1, 1 << 20), (8, 64 << 20)]
+    hold = [(200, 2 << 20), (1200, 4 << 20), (2, 32 << 20)]
 
     def records(sh, seed):
         recs = []

@@ -73,7 +73,7 @@ class BatchConfig(C.Structure):
 
 DEC_T1_ENTRIES = 2048
 DEC_T2_ENTRIES = 2560
-MLP_IN, MLP_HIDDEN, MLP_OUT = 9, 32, 2
+MLP_IN, MLP_HIDDEN, MLP_OUT = 10, 32, 2
 MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_OUT * MLP_HIDDEN + MLP_OUT
 
 

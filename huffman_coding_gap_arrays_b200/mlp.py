@@ -3,7 +3,8 @@ project's own CUDA kernels (csrc/mlp.cu), that predicts how the batched
 compress and decompress times of an input (a batch of buffers, or one buffer)
 move with the launch shape.
 
-    X = [log2 size, entropy, longest code, level-2 byte fraction,        (input)
+    X = [log2 size, entropy, longest code, level-2 byte fraction,
+         log2 buffer count,                                              (input)
          log2 region chunks, histogram / encoder / decoder CTAs per SM,
          decoder tile (-1: 256 segments, 0: by the book, 1: 512)]          (shape)
     y = [log compress ms, log decompress ms], each relative to the mean over
@@ -30,7 +31,7 @@ from .batch import LaunchConfig
 from .codec import _stream
 from .tuner import DEC_SPACE, Autotuner, compress_space, with_dec
 
-SHAPES = [(32, 9), (32,), (32, 32), (32,), (2, 32), (2,)]
+SHAPES = [(32, 10), (32,), (32, 32), (32,), (2, 32), (2,)]
 # CTAs per SM that "0" (the occupancy maximum) means for each grid on B200
 MAX_CTAS = {"hist": 4, "enc": 2, "dec": 4}
 
@@ -47,7 +48,7 @@ def config_vector(cfg: LaunchConfig) -> np.ndarray:
 
 
 def records_to_xy(records, relative: bool = True):
-    """Autotuner records -> (X n x 9, T n x 2 log-ms targets, NaN = not
+    """Autotuner records -> (X n x 10, T n x 2 log-ms targets, NaN = not
     measured).  With `relative`, each target is taken relative to the mean
     log time of the records with the same features (one tuned input)."""
     X = np.stack([np.concatenate([r.features, config_vector(r.config)]) for r in records]).astype(np.float32)
@@ -204,10 +205,10 @@ class LearnedTuner:
         self._memo[key] = pick
         return pick
 
-    def precompute(self, traffic, log2_lo: float, log2_hi: float) -> None:
+    def precompute(self, traffic, log2_lo: float, log2_hi: float, log2_count: float = 0.0) -> None:
         """Fills the memo for every input size from 2^log2_lo to 2^log2_hi (in
-        the memo's 1/8 steps) for fixed byte statistics, with one forward pass
-        per network -- so that a serving loop never waits for one."""
+        the memo's 1/8 steps) for fixed byte statistics and buffer count, with
+        one forward pass per network -- so that a serving loop never waits for one."""
         keys = np.arange(np.floor(log2_lo * 8) / 8, np.ceil(log2_hi * 8) / 8 + 1e-9, 0.125)
         if not len(keys) or not self.mlps:
             return
@@ -215,27 +216,34 @@ class LearnedTuner:
         comp = list(self.space)
         d0dec = (d0.dec_ctas_per_sm, d0.dec_tile_segs)
         base = with_dec(d0, d0dec)
-        feats = [np.round(np.concatenate([[k], np.asarray(traffic, np.float32)]) * 8) / 8 for k in keys]
-        # stage 1: the compress shape for every size at once
-        X = np.stack([np.concatenate([f, config_vector(c)]) for f in feats for c in comp + [base]])
-        P = np.stack([m.predict(X)[:, 0] for m in self.mlps]).reshape(len(self.mlps), len(feats), len(comp) + 1)
-        picks = []
-        for j in range(len(feats)):
-            rel = P[:, j, :-1] - P[:, j, -1:]
+        rest = np.round(np.concatenate([np.asarray(traffic, np.float32), [log2_count]]) * 8) / 8
+        feats = np.concatenate([keys[:, None], np.tile(rest, (len(keys), 1))], axis=1).astype(np.float32)
+        nf = len(feats)
+
+        def rows(cfg_vecs):  # every feature row against every config row (per feature, in order)
+            k = cfg_vecs.shape[-2]
+            F = np.repeat(feats, k, axis=0)
+            Cv = cfg_vecs.reshape(-1, cfg_vecs.shape[-1]) if cfg_vecs.ndim == 3 else np.tile(cfg_vecs, (nf, 1))
+            return np.concatenate([F, Cv], axis=1)
+
+        def best(P, k, margin):  # per feature row: the candidate index, or k (the default)
+            rel = P[:, :, :k] - P[:, :, k:k + 1]
             mean = np.where((rel < 0).all(axis=0), rel.mean(axis=0), np.inf)
-            i = int(np.argmin(mean))
-            picks.append(comp[i] if mean[i] < math.log(1.0 - self.margin) else base)
+            i = np.argmin(mean, axis=1)
+            return np.where(mean[np.arange(nf), i] < math.log(1.0 - margin), i, k)
+
+        # stage 1: the compress shape for every size at once
+        cands = comp + [base]
+        V = np.stack([config_vector(c) for c in cands])
+        P = np.stack([m.predict(rows(V))[:, 0] for m in self.mlps]).reshape(len(self.mlps), nf, len(cands))
+        picks = [cands[i] for i in best(P, len(comp), self.margin)]
         # stage 2: the decoder grid for each size's compress shape
         dec = [[with_dec(c, d) for d in self.dec_space] + [with_dec(c, d0dec)] for c in picks]
-        X = np.stack([np.concatenate([f, config_vector(c)]) for f, row in zip(feats, dec) for c in row])
+        V = np.stack([np.stack([config_vector(c) for c in row]) for row in dec])
         nd = len(self.dec_space) + 1
-        P = np.stack([m.predict(X)[:, 1] for m in self.mlps]).reshape(len(self.mlps), len(feats), nd)
-        for j, f in enumerate(feats):
-            rel = P[:, j, :-1] - P[:, j, -1:]
-            mean = np.where((rel < 0).all(axis=0), rel.mean(axis=0), np.inf)
-            i = int(np.argmin(mean))
-            self._memo[tuple(f.astype(np.float32).tolist())] = (
-                dec[j][i] if mean[i] < math.log(1.0 - self.dec_margin) else dec[j][-1])
+        P = np.stack([m.predict(rows(V))[:, 1] for m in self.mlps]).reshape(len(self.mlps), nf, nd)
+        for j, i in enumerate(best(P, nd - 1, self.dec_margin)):
+            self._memo[tuple(feats[j].tolist())] = dec[j][i]
 
     def choose_or_search(self, features, inputs, outputs) -> LaunchConfig:
         """The ensemble's pick when it is trained and accurate enough on

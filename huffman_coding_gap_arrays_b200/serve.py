@@ -100,8 +100,8 @@ class EncodedStream:
 
 # The batch features the tuner sees in serving, on a coarse grid: log2 bytes in
 # 1/8 steps, code bits per byte to a whole bit, the longest code in three bands
-# (11 or less: no level-2 lookups; 12-13; 14 and up) and the level-2 share as
-# none or some.  The server fills the tuner's memo for the whole grid before the
+# (11 or less: no level-2 lookups; 12-13; 14 and up), the level-2 share as
+# none or some, and log2 of the request count to a whole step.  The server fills the tuner's memo for the whole grid before the
 # clock starts, so no batch waits for a forward pass.
 FEATURE_ENTROPY = tuple(float(e) for e in range(0, 9))
 FEATURE_MAXLEN = (11.0, 13.0, 16.0)
@@ -114,7 +114,8 @@ def quantize_features(f) -> np.ndarray:
     ent = float(np.clip(np.round(f[1]), 0, 8))
     maxlen = 11.0 if f[2] <= 11 else (13.0 if f[2] <= 13 else 16.0)
     l2 = 0.0 if f[3] < 0.0625 else 0.125
-    return np.array([size, ent, maxlen, l2], np.float32)
+    count = float(np.clip(np.round(f[4]), 0, 16)) if f.size > 4 else 0.0
+    return np.array([size, ent, maxlen, l2, count], np.float32)
 
 
 ALLOC_GRAIN = 512  # the caching allocator rounds every block up to a multiple of this
@@ -155,6 +156,7 @@ class _Batch:
     plan: BatchCodec | None = None
     dec_ws: torch.Tensor | None = None
     status_host: torch.Tensor | None = None  # the workspaces' status words, copied after the launches
+    shape: str = ""                          # its launch shape, for the per-shape statistics
 
 
 class Server:
@@ -193,6 +195,7 @@ class Server:
         self.slot_waits = 0       # loop passes with requests ready but every slot busy
         self.bound_misses = 0     # batches that allocated more than their admission bound
         self.tuner_misses = 0     # batches whose launch shape needed a forward pass of the tuner
+        self.shapes = {}          # launch shape -> [batches, bytes, summed service seconds]
         # a batch's fixed part per kind: the workspace header, and the allocator's
         # rounding of each of its shared tensors (8 for compress, 3 for decompress)
         L = lib()
@@ -205,6 +208,7 @@ class Server:
         """Zeroes the statistics (after a warm-up run)."""
         self.batches = self.peak_held = self.mem_waits = self.slot_waits = self.bound_misses = 0
         self.tuner_misses = 0
+        self.shapes = {}
 
     # --------------------------------------------------------------- memory
     def request_bytes(self, r: Request) -> int:
@@ -243,7 +247,7 @@ class Server:
         acc = np.zeros(3, np.float64)
         for r in reqs:
             acc += r.nbytes * (r.stream.features if r.kind == "decompress" else self.traffic)
-        return quantize_features(np.concatenate([[np.log2(total)], acc / total]))
+        return quantize_features(np.concatenate([[np.log2(total)], acc / total, [np.log2(len(reqs))]]))
 
     def _config_for(self, reqs) -> LaunchConfig:
         if self.tuner is None:
@@ -265,6 +269,8 @@ class Server:
         before = _allocated(self.device)
         b = _Batch(reqs, s, torch.cuda.Event(), 0)
         cfg = self._config_for(reqs)
+        b.shape = (f"r{cfg.region_chunks}/h{cfg.hist_ctas_per_sm}/e{cfg.enc_ctas_per_sm}"
+                   f"/d{cfg.dec_ctas_per_sm}/t{cfg.dec_tile_segs}")
         comp = [r for r in reqs if r.kind == "compress"]
         dec = [r for r in reqs if r.kind == "decompress"]
         # Allocations and uploads on the current stream: the caching allocator keeps one
@@ -349,6 +355,10 @@ class Server:
             check(lib().hgap_status_from_word(words[1] & 0xffffffff), "served decompress")
         for r in b.reqs:
             r.done = now
+        st = self.shapes.setdefault(b.shape, [0, 0, 0.0])
+        st[0] += 1
+        st[1] += sum(r.nbytes for r in b.reqs)
+        st[2] += now - b.reqs[0].start
         self.free_streams.append(b.stream)
         if b.plan is not None:
             comp = [r for r in b.reqs if r.kind == "compress"]
@@ -382,7 +392,8 @@ class Server:
             for e in FEATURE_ENTROPY:
                 for m in FEATURE_MAXLEN:
                     for l2 in FEATURE_L2:
-                        self.tuner.precompute(np.array([e, m, l2], np.float32), lo, hi)
+                        for k in range(int(np.round(np.log2(self.max_batch))) + 1):
+                            self.tuner.precompute(np.array([e, m, l2], np.float32), lo, hi, float(k))
         # the cyclic garbage collector stays off while the clock runs: a full pass over
         # the run's objects stalled a launch for ~100 ms and every request queued behind it
         gc_on = gc.isenabled()
@@ -464,7 +475,15 @@ class Server:
                 "service_p99_ms": round(float(np.percentile(svc, 99)), 3), "batches": self.batches,
                 "peak_hbm_gb": round(self.peak_held / 1e9, 3), "budget_gb": round(self.budget / 1e9, 3),
                 "mem_waits": self.mem_waits, "slot_waits": self.slot_waits,
-                "bound_misses": self.bound_misses, "tuner_misses": self.tuner_misses}
+                "bound_misses": self.bound_misses, "tuner_misses": self.tuner_misses,
+                "shapes": self._shape_stats()}
+
+    def _shape_stats(self) -> dict:
+        """The launch shapes the batches took (region chunks / histogram,
+        encoder, decoder CTAs per SM / decoder tile), most used first: batches,
+        mean MB per batch, mean service ms."""
+        top = sorted(self.shapes.items(), key=lambda kv: -kv[1][0])[:8]
+        return {k: [v[0], round(v[1] / v[0] / 1e6, 2), round(1e3 * v[2] / v[0], 3)] for k, v in top}
 
 
 def poisson_requests(count: int, rate_gbs: float, pool: torch.Tensor, streams: list, seed: int = 5,

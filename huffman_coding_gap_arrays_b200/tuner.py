@@ -12,7 +12,8 @@ Features of a buffer (cheap, from its histogram and codebook):
   the fraction of its bytes whose code is longer than the decoder's 11-bit
   level-1 prefix (level-2 lookups, the decoder's slow path).  A batch has the
   same four, over all its bytes: log2 of its total size and the byte-weighted
-  means of the other three.
+  means of the other three; and a fifth, log2 of its buffer count (0 for one
+  buffer), which tells one 64 MiB buffer from 4096 buffers of 16 KiB.
 """
 from __future__ import annotations
 
@@ -62,10 +63,10 @@ def buffer_features(x: torch.Tensor) -> np.ndarray:
     from . import codec
     n = x.numel()
     if n == 0:
-        return np.zeros(4, np.float32)
+        return np.zeros(5, np.float32)
     hist = codec.histogram(x).cpu().numpy().view(np.uint32)
     book, _ = codec.Codebook.from_histogram(hist)
-    return features_from_hist(n, hist, book.length)
+    return np.concatenate([features_from_hist(n, hist, book.length), [0.0]]).astype(np.float32)
 
 
 def batch_features(inputs) -> np.ndarray:
@@ -74,7 +75,7 @@ def batch_features(inputs) -> np.ndarray:
     sizes = [int(t.numel()) for t in inputs]
     total = sum(sizes)
     if total == 0:
-        return np.zeros(4, np.float32)
+        return np.zeros(5, np.float32)
     hs = torch.stack([torch.bincount(t, minlength=256) if t.numel() else
                       torch.zeros(256, dtype=torch.int64, device=t.device) for t in inputs]).cpu().numpy()
     acc = np.zeros(3)
@@ -84,7 +85,7 @@ def batch_features(inputs) -> np.ndarray:
         book, _ = codec.Codebook.from_histogram(h.astype(np.uint32))
         f = features_from_hist(n, h, book.length)
         acc += n * f[1:]
-    return np.concatenate([[math.log2(total)], acc / total]).astype(np.float32)
+    return np.concatenate([[math.log2(total)], acc / total, [math.log2(len(sizes))]]).astype(np.float32)
 
 
 @dataclass

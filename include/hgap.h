@@ -321,16 +321,16 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
 hgap_status hgap_batch_status(const void* d_workspace, hgap_stream_t stream);
 
 /* --------------------------------------------------------- learned launch tuner
- * No counterpart in the reference.  A small MLP (9 inputs -> 32 ReLU -> 32
+ * No counterpart in the reference.  A small MLP (10 inputs -> 32 ReLU -> 32
  * ReLU -> 2 outputs, fp32) that predicts the log times of the batched
  * compress and decompress from a batch's features and a launch shape,
  * trained and run on the GPU by these kernels.  Parameters: one flat array of
- * HGAP_MLP_PARAMS floats, W1[32][9] b1[32] W2[32][32] b2[32] W3[2][32] b3[2].
- * d_x: n x 8 inputs, d_y / d_target: n x 2 (NaN targets are unmeasured and
+ * HGAP_MLP_PARAMS floats, W1[32][10] b1[32] W2[32][32] b2[32] W3[2][32] b3[2].
+ * d_x: n x 10 inputs, d_y / d_target: n x 2 (NaN targets are unmeasured and
  * carry no loss).  loss = scale * sum (y - t)^2 / 2; hgap_mlp_loss_grad
  * overwrites d_grad (HGAP_MLP_PARAMS floats) and *d_loss.  Adam with bias
  * correction for step >= 1, on the gradient plus weight_decay * params. */
-#define HGAP_MLP_IN 9
+#define HGAP_MLP_IN 10
 #define HGAP_MLP_HIDDEN 32
 #define HGAP_MLP_OUT 2
 #define HGAP_MLP_PARAMS (HGAP_MLP_HIDDEN * HGAP_MLP_IN + HGAP_MLP_HIDDEN + HGAP_MLP_HIDDEN * HGAP_MLP_HIDDEN + \

@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import numpy as np
 
-IN, HID, OUT = 9, 32, 2
+IN, HID, OUT = 10, 32, 2
 SHAPES = [("W1", (HID, IN)), ("b1", (HID,)), ("W2", (HID, HID)), ("b2", (HID,)), ("W3", (OUT, HID)),
           ("b3", (OUT,))]
 PARAMS = sum(int(np.prod(s)) for _, s in SHAPES)
