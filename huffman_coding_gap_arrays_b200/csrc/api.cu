@@ -31,7 +31,7 @@ hgap_status hgap_histogram(const void* d_in, uint64_t n, uint32_t* d_hist, hgap_
 }
 
 size_t hgap_encode_workspace_bytes(uint64_t n) {
-    const uint64_t nst = hgap::encode_super_tiles(n + 15, n);  // worst case over alignments
+    const uint64_t nst = hgap::encode_super_tiles_cap(n);  // every input of up to n bytes, any alignment
     return hgap::kEncWsHeader + (size_t)nst * (sizeof(uint64_t) + 256 * sizeof(uint32_t));
 }
 

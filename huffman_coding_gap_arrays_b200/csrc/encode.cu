@@ -235,32 +235,47 @@ __global__ void __launch_bounds__(kEncThreads, 2)
                 if (nibs && gs + 127 < stop) stop = gs + 127;
                 uint64_t end = G;
                 const uint64_t vfirst = st * (uint64_t)J.st_bytes;  // first byte of this region
-                for (uint64_t base = 0;; base += 32) {
-                    const uint64_t v = vfirst - 1 - base - lane;     // may wrap below lo: no byte
-                    uint32_t c = 0, len = 0;
-                    if (vfirst >= base + lane + 1 && v >= J.lo) {
-                        const uint32_t byte = __ldg(J.in_aligned + v);
-                        if (a.jobs) {
-                            code_of(a.tables + jid, byte, c, len);
-                        } else {
-                            c = lutc[(byte << 5) | lane];
-                            len = lutl[(byte << 5) | lane] & 31u;
+                // 32 bytes a step, one per lane, going backwards; the bytes of kWalkAhead
+                // steps are loaded at once (one memory round trip, not one per step)
+                constexpr int kWalkAhead = 4;
+                for (uint64_t base0 = 0;; base0 += 32 * kWalkAhead) {
+                    uint32_t pre[kWalkAhead];
+#pragma unroll
+                    for (int k = 0; k < kWalkAhead; ++k) {
+                        const uint64_t base = base0 + 32 * k;
+                        const uint64_t v = vfirst - 1 - base - lane;  // may wrap below lo: no byte
+                        pre[k] = (vfirst >= base + lane + 1 && v >= J.lo) ? (uint32_t)__ldg(J.in_aligned + v) : 0x100u;
+                    }
+                    bool done = false;  // warp-uniform
+#pragma unroll
+                    for (int k = 0; k < kWalkAhead; ++k) {
+                        if (done) break;
+                        uint32_t c = 0, len = 0;
+                        if (pre[k] < 0x100u) {
+                            const uint32_t byte = pre[k];
+                            if (a.jobs) {
+                                code_of(a.tables + jid, byte, c, len);
+                            } else {
+                                c = lutc[(byte << 5) | lane];
+                                len = lutl[(byte << 5) | lane] & 31u;
+                            }
                         }
+                        const uint32_t incl = warp_incl_scan(len, lane);
+                        const uint64_t ce = end - (incl - len);  // this code's end bit
+                        const uint64_t cs = ce - len;            // and start bit
+                        if (len) {
+                            if (r && ce > wstart)  // the code's right-aligned value, placed to end at ce
+                                head |= (uint32_t)(((uint64_t)(c >> (32 - len))) << (wstart + 32 - ce));
+                            const uint64_t b = (ce >> 7) << 7;   // last segment boundary <= end
+                            if (nibs && b > cs && b >= gs + 128)
+                                gcarry |= (uint32_t)(ce - b) << (4 * (uint32_t)(((b >> 7) - 1) & 7));
+                        }
+                        const uint32_t total = __shfl_sync(kFull, incl, 31);
+                        const uint64_t smin = end - total;  // start of the step's last code
+                        end = smin;
+                        if (smin <= stop || total == 0) done = true;
                     }
-                    const uint32_t incl = warp_incl_scan(len, lane);
-                    const uint64_t ce = end - (incl - len);  // this code's end bit
-                    const uint64_t cs = ce - len;            // and start bit
-                    if (len) {
-                        if (r && ce > wstart)  // the code's right-aligned value, placed to end at ce
-                            head |= (uint32_t)(((uint64_t)(c >> (32 - len))) << (wstart + 32 - ce));
-                        const uint64_t b = (ce >> 7) << 7;   // last segment boundary <= end
-                        if (nibs && b > cs && b >= gs + 128)
-                            gcarry |= (uint32_t)(ce - b) << (4 * (uint32_t)(((b >> 7) - 1) & 7));
-                    }
-                    const uint32_t total = __shfl_sync(kFull, incl, 31);
-                    const uint64_t smin = end - total;  // start of the batch's last code
-                    end = smin;
-                    if (smin <= stop || total == 0) break;
+                    if (done) break;
                 }
                 head = __reduce_or_sync(kFull, head);
                 gcarry = __reduce_or_sync(kFull, gcarry);

@@ -17,6 +17,7 @@ Features of a buffer (cheap, from its histogram and codebook):
 """
 from __future__ import annotations
 
+import ctypes as C
 import itertools
 import math
 from dataclasses import dataclass, field
@@ -70,21 +71,37 @@ def buffer_features(x: torch.Tensor) -> np.ndarray:
 
 
 def batch_features(inputs) -> np.ndarray:
-    """Features of a batch of uint8 CUDA buffers (histograms on the device)."""
+    """Features of a batch of uint8 CUDA buffers: the histograms by this
+    library's histogram kernel, the codebooks by its device builder (one warp
+    per histogram), the per-buffer statistics vectorised over the batch."""
     from . import codec
-    sizes = [int(t.numel()) for t in inputs]
-    total = sum(sizes)
+    from ._lib import CCodebook, check, lib
+    sizes = np.array([int(t.numel()) for t in inputs], np.int64)
+    total = int(sizes.sum())
     if total == 0:
         return np.zeros(5, np.float32)
-    hs = torch.stack([torch.bincount(t, minlength=256) if t.numel() else
-                      torch.zeros(256, dtype=torch.int64, device=t.device) for t in inputs]).cpu().numpy()
-    acc = np.zeros(3)
-    for n, h in zip(sizes, hs):
-        if n == 0:
-            continue
-        book, _ = codec.Codebook.from_histogram(h.astype(np.uint32))
-        f = features_from_hist(n, h, book.length)
-        acc += n * f[1:]
+    dev = next(t.device for t in inputs if t.numel())
+    hs = torch.zeros((len(inputs), 256), dtype=torch.int32, device=dev)
+    for i, t in enumerate(inputs):
+        if t.numel():
+            codec.histogram(t, out=hs[i])
+    books = torch.empty(len(inputs) * C.sizeof(CCodebook), dtype=torch.uint8, device=dev)
+    bsizes = torch.empty(len(inputs) * 4, dtype=torch.int64, device=dev)
+    check(lib().hgap_codebook_build_device(len(inputs), hs.data_ptr(), books.data_ptr(), bsizes.data_ptr(),
+                                           codec._stream(None)), "hgap_codebook_build_device")
+    h = hs.cpu().numpy().view(np.uint32).astype(np.float64)
+    # per-byte code lengths: hgap_codebook.table[b].length
+    off = CCodebook.table.offset
+    raw = books.cpu().numpy().reshape(len(inputs), C.sizeof(CCodebook))[:, off:off + 8 * 256]
+    lens = np.ascontiguousarray(raw).view(np.uint32).reshape(len(inputs), 256, 2)[:, :, 1].astype(np.float64)
+    n = h.sum(axis=1)
+    ok = n > 0
+    p = np.where(h > 0, h / np.maximum(n, 1)[:, None], 1.0)
+    ent = -(np.where(h > 0, p * np.log2(p), 0.0)).sum(axis=1)
+    maxlen = np.where(h > 0, lens, 0.0).max(axis=1)
+    l2 = np.where(lens > 11, h, 0.0).sum(axis=1) / np.maximum(n, 1)
+    w = np.where(ok, sizes, 0).astype(np.float64)
+    acc = np.array([(w * ent).sum(), (w * maxlen).sum(), (w * l2).sum()])
     return np.concatenate([[math.log2(total)], acc / total, [math.log2(len(sizes))]]).astype(np.float32)
 
 

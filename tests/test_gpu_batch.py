@@ -290,3 +290,23 @@ def test_batch_bf16_planes():
         ref = H.compress(x)
         got = plan.stream(i)
         assert torch.equal(got.bits, ref.bits) and torch.equal(got.gaps, ref.gaps)
+
+
+def test_batch_features_match_per_buffer_host_books():
+    """tuner.batch_features (device histograms and codebooks, vectorised)
+    equals the per-buffer statistics from host codebooks."""
+    import math
+    from huffman_coding_gap_arrays_b200 import tuner as TU
+    sizes = [0, 1, 300, 4096, 70000, 1 << 20]
+    bufs = _make_buffers(sizes, 62)
+    bufs[2] = torch.full((300,), 7, dtype=torch.uint8, device="cuda")  # one symbol
+    f = TU.batch_features(bufs)
+    acc, total = np.zeros(3), sum(sizes)
+    for x in bufs:
+        if x.numel() == 0:
+            continue
+        h = H.histogram(x).cpu().numpy().view(np.uint32)
+        book, _ = H.Codebook.from_histogram(h)
+        acc += x.numel() * TU.features_from_hist(x.numel(), h, book.length)[1:]
+    want = np.concatenate([[math.log2(total)], acc / total, [math.log2(len(sizes))]])
+    assert np.allclose(f, want, rtol=1e-5, atol=1e-6), (f, want)
