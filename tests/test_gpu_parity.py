@@ -138,6 +138,24 @@ def test_reused_workspace_and_side_stream(cuda):
         assert np.array_equal(y.cpu().numpy(), x)
 
 
+@pytest.mark.parametrize("cap_chunks,n_chunks", [(300, 296), (600, 592), (9500, 9400)])
+def test_workspace_for_capacity_serves_smaller_inputs(cuda, cap_chunks, n_chunks):
+    """An encoder workspace sized for `capacity` bytes takes any smaller input,
+    also one the super-tile rule splits into more super-tiles than the
+    capacity itself (296 chunks: 296 one-chunk super-tiles; 300 chunks: 150
+    two-chunk ones), at every alignment."""
+    cap = cap_chunks * 8192 - 100
+    enc = H.Encoder(cap)
+    for off in (0, 5):
+        n = n_chunks * 8192 - 100 - off
+        x = make("zipf", n, n_chunks + off)
+        h = O.histogram(x)
+        book, sizes = H.Codebook.from_histogram(h)
+        bits, gaps = enc.encode(to_dev(x, off), book, sizes)
+        bits_o, gaps_o, _ = O.encode(x, O.codebook(h))
+        assert np.array_equal(u32(bits), bits_o) and np.array_equal(u32(gaps), gaps_o)
+
+
 def test_compress_container_round_trip(cuda):
     x = make("zipf", 777_777, 9)
     c = H.compress(to_dev(x))
