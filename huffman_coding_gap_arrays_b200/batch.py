@@ -89,11 +89,19 @@ class BatchCodec:
         self.bits_capacity = int(L.hgap_batch_bits_capacity(self.count, _u64p(self.sizes)))
         self.gaps_capacity = int(L.hgap_batch_gaps_capacity(self.count, _u64p(self.sizes)))
         dev = self.device
-        self.enc_ws = torch.empty((enc_ws + 7) // 8, dtype=torch.int64, device=dev)
-        self.dec_ws = torch.empty((dec_ws + 7) // 8, dtype=torch.int64, device=dev)
-        self.bits = torch.empty(max(self.bits_capacity, 4), dtype=torch.int32, device=dev)
-        self.gaps = torch.empty(max(self.gaps_capacity, 1), dtype=torch.int32, device=dev)
-        self.entries = torch.zeros(max(self.count, 1) * ENTRY_BYTES, dtype=torch.uint8, device=dev)
+        # one device allocation carved into the workspaces, arenas and entries (256-byte aligned)
+        parts = [("enc_ws", enc_ws, torch.int64), ("dec_ws", dec_ws, torch.int64),
+                 ("bits", 4 * max(self.bits_capacity, 4), torch.int32),
+                 ("gaps", 4 * max(self.gaps_capacity, 1), torch.int32),
+                 ("entries", max(self.count, 1) * ENTRY_BYTES, torch.uint8)]
+        offs, total = [], 0
+        for _, nbytes, dt in parts:
+            offs.append(total)
+            total += (nbytes + 255) & ~255
+        self._arena = torch.empty(total, dtype=torch.uint8, device=dev)
+        for (name, nbytes, dt), o in zip(parts, offs):
+            setattr(self, name, self._arena[o:o + (nbytes + dt.itemsize - 1) // dt.itemsize * dt.itemsize].view(dt))
+        self.entries.zero_()
         # sizes, input pointers and output pointers in one device array, uploaded at once
         k = max(self.count, 1)
         meta = np.zeros(3 * k, np.int64)

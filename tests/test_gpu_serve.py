@@ -86,7 +86,25 @@ def test_request_bound_covers_real_allocations():
         b.event.synchronize()
         assert 0 < b.reserved <= server._bound(reqs)
         server._retire(b, 0.0)
+    # one decompress request alone takes the single-buffer decoder
+    r = SV.Request(9, 0.0, "decompress", stream=streams[0])
+    torch.cuda.synchronize()
+    b = server._launch([r], 0.0)
+    server.held += b.reserved
+    b.event.synchronize()
+    assert 0 < b.reserved <= server._bound([r])
+    server._retire(b, 0.0)
+    assert torch.equal(r.result, bufs[0])
     assert server.held == 0
+
+
+def test_light_load_single_requests():
+    """At a light load most batches hold one request (a lone decompress goes
+    through the single-buffer decoder); every result is still exact."""
+    server = SV.Server(keep_results=True)
+    stats, reqs = _run(server, 24, 1.0, seed=15, hi=2 << 20)
+    assert stats["batches"] >= 12
+    assert {r.kind for r in reqs} == {"compress", "decompress"}
 
 
 def test_learned_tuner_policy_and_fixed_shape_agree():
