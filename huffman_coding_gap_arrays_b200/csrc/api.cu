@@ -211,9 +211,6 @@ hgap_status decode_impl(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     hgap_status s = canonical_copy(cb, &book);
     if (s != HGAP_OK) return s;
     if (book.symbol_count == 0) return HGAP_ERR_CORRUPT;
-    hgap::DecTable t;
-    s = hgap::make_dec_table(book, &t);
-    if (s != HGAP_OK) return s;
     uint32_t min_len = hgap::kMaxLen;
     uint64_t kraft = 0;  // units of 2^-16; a complete book (sum 1) has no invalid table entry
     for (uint32_t i = 0; i < book.symbol_count; ++i) {
@@ -244,7 +241,11 @@ hgap_status decode_impl(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     a.counter = reinterpret_cast<uint32_t*>(ws) + 1;
     a.lookback = reinterpret_cast<uint64_t*>(ws + kWsHeader);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    // the workspace is cleared on the device while the host builds the table
     if (cudaMemsetAsync(ws, 0, need, st) != cudaSuccess) return HGAP_ERR_CUDA;
+    hgap::DecTable t;
+    s = hgap::make_dec_table(book, &t);
+    if (s != HGAP_OK) return s;
     const bool complete = kraft == (1ull << hgap::kMaxLen);
     // two symbols per lookup pay off once about a third of the lookups yield two
     const bool pairs = hgap::dec_pair_fraction(t) >= 0.3;
