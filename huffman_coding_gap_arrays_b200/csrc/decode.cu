@@ -60,10 +60,11 @@ struct DecCfg {
     static constexpr int kRow = 4 * kRowWords;
     static constexpr int kStageBytes = kSegs * kRow + 16;
     static constexpr int kCompactBytes = kSegs * kMaxSym + 64;
-    static constexpr int kL1Bytes = dec_multi(R, true) ? kT1 : 0;  // multi entries: first-code lengths
     // the level-2 table stays in global memory (or the kernel parameter): codes longer
-    // than the 11-bit prefix are rare, and its shared memory buys CTAs per SM
-    static constexpr size_t kSmem = (size_t)(kT1 + kGapStage) * 4 + kStageBytes + kCompactBytes + kL1Bytes;
+    // than the 11-bit prefix are rare, and its shared memory buys CTAs per SM; so do
+    // the multi entries' first-code lengths (read only where a multi entry would run
+    // past the segment: 2 KiB less takes the 32-row decoder from 2 to 3 CTAs per SM)
+    static constexpr size_t kSmem = (size_t)(kT1 + kGapStage) * 4 + kStageBytes + kCompactBytes;
     // CTAs per SM the shared memory allows (227 KiB usable, ~1.5 KiB static and
     // reserved per CTA), at most 4 (64 registers a thread)
     static constexpr int kBySmem = (int)((227u * 1024u) / (kSmem + 1536u));
@@ -81,6 +82,18 @@ __device__ __forceinline__ uint32_t lookup(const uint32_t* t1, const uint16_t* _
     }
     return e;
 }
+
+// Length of the first code of a multi entry's prefix: from the widened table's
+// byte array in global memory (batched path) or derived from the u16 level-1
+// table in the kernel parameter (single path).
+struct FirstLen {
+    const uint8_t* g;
+    const uint16_t* t1src;
+    __device__ __forceinline__ uint32_t operator()(uint32_t x) const {
+        const uint32_t i = x >> (32 - kDecPrefix);
+        return g ? (uint32_t)__ldg(g + i) : (uint32_t)first_len(t1src, i);
+    }
+};
 
 // The words of one segment in registers: its own four and the next segment's
 // first (a code that starts in the segment may end up to 15 bits into it).
@@ -100,7 +113,7 @@ struct SegWords {
 // after an invalid code) and advances `out` past the symbols.
 template <bool COMPLETE, bool PAIRS, bool MULTI>
 __device__ __forceinline__ uint32_t decode_segment(const uint32_t* t1, const uint16_t* __restrict__ t2,
-                                                   const uint8_t* l1t, const SegWords& w, uint32_t pos,
+                                                   const FirstLen& fl, const SegWords& w, uint32_t pos,
                                                    uint8_t*& out) {
     constexpr uint32_t kBad = 1u << 16;  // position after an invalid code: every loop ends
     auto run_fast = [&](uint32_t cw, uint32_t nw, uint32_t stop) {
@@ -155,7 +168,7 @@ __device__ __forceinline__ uint32_t decode_segment(const uint32_t* t1, const uin
                 pos += tot;
             } else {
                 out += 1;
-                pos += more ? (uint32_t)l1t[x >> (32 - kDecPrefix)] : tot;
+                pos += more ? fl(x) : tot;
             }
         } else {
             const uint32_t tot = e >> 24;
@@ -176,7 +189,7 @@ __device__ __forceinline__ uint32_t decode_segment(const uint32_t* t1, const uin
 // any pair or multi entry), the words picked by index.
 template <bool COMPLETE, bool PAIRS, bool MULTI>
 __device__ __forceinline__ uint32_t decode_last_segment(const uint32_t* t1, const uint16_t* __restrict__ t2,
-                                                        const uint8_t* l1t, const SegWords& w, uint32_t pos,
+                                                        const FirstLen& fl, const SegWords& w, uint32_t pos,
                                                         uint32_t end, uint8_t* out) {
     auto word = [&](uint32_t i) { return i == 0 ? w.w0 : i == 1 ? w.w1 : i == 2 ? w.w2 : i == 3 ? w.w3 : w.w4; };
     uint32_t cnt = 0;
@@ -187,7 +200,7 @@ __device__ __forceinline__ uint32_t decode_last_segment(const uint32_t* t1, cons
         if (!COMPLETE && (e & 0x40000000u)) break;  // the padding after the final codeword
         uint32_t len;
         if (MULTI) {
-            len = ((e >> 29) & 3u) ? (uint32_t)l1t[x >> (32 - kDecPrefix)] : ((e >> 24) & 31u);
+            len = ((e >> 29) & 3u) ? fl(x) : ((e >> 24) & 31u);
         } else if (PAIRS) {
             len = (e & 0x10000u) ? ((e >> 17) & 15u) : (e >> 24);
         } else {
@@ -222,7 +235,6 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R, SEGS>::kMinBlocks)
     uint32_t* sg = smem + C::kT1;                         // gap words: sg[j] = gaps[s0/8 - 1 + j]
     uint8_t* stage = reinterpret_cast<uint8_t*>(sg + C::kGapStage);
     uint8_t* compact = stage + C::kStageBytes;
-    uint8_t* l1t = compact + C::kCompactBytes;            // multi entries: length of the first code
     __shared__ uint32_t warp_tot[C::kWarps];
     __shared__ DecSlot slot[3];  // ring: the tile being decoded, the next one, the previous one
     __shared__ uint64_t s_O;
@@ -236,7 +248,6 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R, SEGS>::kMinBlocks)
         for (int i = tid; i < C::kT1; i += kDecThreads) {
             if (MULTI) {
                 t1[i] = widen_multi(t.t1, i);
-                l1t[i] = first_len(t.t1, i);
             } else {
                 t1[i] = PAIRS ? widen_pair(t.t1, i) : widen_entry(t.t1[i]);
             }
@@ -246,10 +257,6 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R, SEGS>::kMinBlocks)
     auto copy_tables = [&](const DecTableW& t) {
         const uint4* s1 = reinterpret_cast<const uint4*>(t.t1);
         for (int i = tid; i < C::kT1 / 4; i += kDecThreads) reinterpret_cast<uint4*>(t1)[i] = s1[i];
-        if (MULTI) {
-            const uint4* sl = reinterpret_cast<const uint4*>(t.l1);
-            for (int i = tid; i < C::kT1 / 16; i += kDecThreads) reinterpret_cast<uint4*>(l1t)[i] = sl[i];
-        }
     };
     // thread 0: the tile `item` and its job into slot s
     auto fill_slot = [&](int s, uint64_t item) {
@@ -323,6 +330,7 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R, SEGS>::kMinBlocks)
         if (tid == 0 && have) claim = atomicAdd(a.counter, 1u);  // its latency hides behind the decode
         const uint64_t s0 = T.local * C::kSegs;  // first segment of the tile within its job
         const uint16_t* const t2 = a.jobs ? a.tables[T.job_id].t2 : tab.t2;  // level 2, not staged
+        const FirstLen fl{a.jobs ? a.tables[T.job_id].l1 : nullptr, tab.t1};
         // tile-local, 32-bit from here on: segments [0, nseg) of the tile; the stream's last
         // segment (if in this tile) ends at bit end_last instead of at its 128-bit boundary
         const uint64_t seg_rem = have ? T.job.segments - s0 : 0;
@@ -352,11 +360,11 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R, SEGS>::kMinBlocks)
                 const uint32_t pos = gap_at(col + 7) & (col ? ~0u : first_gap);
                 uint8_t* const row = stage + col * C::kRow;
                 if (last_tile && col + 1 == nseg) {
-                    cnt = decode_last_segment<COMPLETE, PAIRS, MULTI>(t1, t2, l1t, w, pos,
+                    cnt = decode_last_segment<COMPLETE, PAIRS, MULTI>(t1, t2, fl, w, pos,
                                                                       end_last - 128 * col, row);
                 } else {
                     uint8_t* out = row;
-                    const uint32_t e = decode_segment<COMPLETE, PAIRS, MULTI>(t1, t2, l1t, w, pos, out);
+                    const uint32_t e = decode_segment<COMPLETE, PAIRS, MULTI>(t1, t2, fl, w, pos, out);
                     cnt = (uint32_t)(out - row);
                     if (e != 32 + gap_at(col + 8)) atomicOr(a.status, kDevCorrupt);
                 }
