@@ -66,9 +66,11 @@ struct DecCfg {
     // past the segment: 2 KiB less takes the 32-row decoder from 2 to 3 CTAs per SM)
     static constexpr size_t kSmem = (size_t)(kT1 + kGapStage) * 4 + kStageBytes + kCompactBytes;
     // CTAs per SM the shared memory allows (227 KiB usable, ~1.5 KiB static and
-    // reserved per CTA), at most 4 (64 registers a thread)
+    // reserved per CTA), at most 5 for 256-segment tiles (48 registers a thread, no
+    // spills) and 4 for 512-segment ones (64 registers: two segments' words in flight)
     static constexpr int kBySmem = (int)((227u * 1024u) / (kSmem + 1536u));
-    static constexpr int kMinBlocks = kBySmem >= 4 ? 4 : (kBySmem < 1 ? 1 : kBySmem);
+    static constexpr int kCap = SEGS == 256 ? 5 : 4;
+    static constexpr int kMinBlocks = kBySmem >= kCap ? kCap : (kBySmem < 1 ? 1 : kBySmem);
     static_assert(kT1 % 4 == 0 && kGapStage % 4 == 0 && kStageBytes % 16 == 0, "16-byte aligned areas");
 };
 
