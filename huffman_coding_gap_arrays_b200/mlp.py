@@ -33,7 +33,7 @@ from .tuner import DEC_SPACE, Autotuner, compress_space, with_dec
 
 SHAPES = [(32, 10), (32,), (32, 32), (32,), (2, 32), (2,)]
 # CTAs per SM that "0" (the occupancy maximum) means for each grid on B200
-MAX_CTAS = {"hist": 4, "enc": 2, "dec": 4}
+MAX_CTAS = {"hist": 4, "enc": 2, "dec": 5}  # what 0 (the occupancy maximum) stands for in the features
 
 
 TILE_CODE = {0: 0.0, 256: -1.0, 512: 1.0}

@@ -30,7 +30,9 @@ from .batch import BatchCodec, LaunchConfig
 REGIONS = (1, 2, 4, 8, 16, 32)
 HIST_CTAS = (2, 4)
 ENC_CTAS = (1, 2)
-DEC_CTAS = (1, 2, 3, 4)  # decoder CTAs per SM; each stage size is clamped to what fits (4, 3 or 2)
+# decoder CTAs per SM; each decoder is clamped to what fits it (5 for 256-segment tiles, 4 for
+# 512-segment ones, 3 for 32 stage rows), and 0 takes that maximum
+DEC_CTAS = (1, 2, 3, 4, 0)
 DEC_TILES = (0, 256, 512)  # decoder tile: by the book's shortest code (0), or 256 / 512 segments for all
 DEC_SPACE = tuple(itertools.product(DEC_CTAS, DEC_TILES))  # (CTAs per SM, tile) pairs
 
