@@ -20,7 +20,8 @@
 //   2. bdec_setup   one CTA: tiles per buffer, look-back record numbering,
 //                   and per class the numbering of the class's tiles;
 //   3. bdec_map     tile -> buffer map of each class;
-//   4. decode       one persistent launch per class (8), the single-buffer
+//   4. decode       one persistent launch per class (all 8, or those the
+//                   caller names in dec_class_mask), the single-buffer
 //                   decoder kernel over the class's tiles.
 // Every launch has a fixed grid and reads its work counts from device memory,
 // so the sequence can be captured once and replayed.
