@@ -100,7 +100,8 @@ class BatchCodec:
             total += (nbytes + 255) & ~255
         self._arena = torch.empty(total, dtype=torch.uint8, device=dev)
         for (name, nbytes, dt), o in zip(parts, offs):
-            setattr(self, name, self._arena[o:o + (nbytes + dt.itemsize - 1) // dt.itemsize * dt.itemsize].view(dt))
+            whole = (nbytes + dt.itemsize - 1) // dt.itemsize * dt.itemsize
+            setattr(self, name, self._arena[o:o + whole].view(dt))
         self.entries.zero_()
         # sizes, input pointers and output pointers in one device array, uploaded at once
         k = max(self.count, 1)

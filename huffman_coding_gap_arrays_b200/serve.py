@@ -109,8 +109,9 @@ class EncodedStream:
 # The batch features the tuner sees in serving, on a coarse grid: log2 bytes in
 # 1/8 steps, code bits per byte to a whole bit, the longest code in three bands
 # (11 or less: no level-2 lookups; 12-13; 14 and up), the level-2 share as
-# none or some, and log2 of the request count to a whole step.  The server fills the tuner's memo for the whole grid before the
-# clock starts, so no batch waits for a forward pass.
+# none or some, and log2 of the request count to a whole step.  The server
+# fills the tuner's memo for the whole grid before the clock starts, so no
+# batch waits for a forward pass.
 FEATURE_ENTROPY = tuple(float(e) for e in range(0, 9))
 FEATURE_MAXLEN = (11.0, 13.0, 16.0)
 FEATURE_L2 = (0.0, 0.125)
