@@ -631,6 +631,7 @@ hgap_status hgap_batch_compress(uint32_t count, const uint8_t* const* d_inputs, 
     h.nitems_dev = nitems;
     h.hist = hists;
     h.st_hist = st_hist;
+    h.counter = status + 2;  // in the zeroed header, beside the encoder's region counter
     if (launch_hist_st(h, (int)cfg->hist_ctas_per_sm, stream) != 0) return HGAP_ERR_CUDA;
 
     if (set_book_smem(book_kernel) != cudaSuccess) return HGAP_ERR_CUDA;

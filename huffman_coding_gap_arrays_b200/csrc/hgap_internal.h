@@ -160,6 +160,7 @@ struct HistStArgs {
     uint32_t* hist;             // [count][256] histograms (zeroed before the launch)
     uint32_t* st_hist;          // [nitems][256]
     uint64_t* tag;              // single path: receives {n, input address}
+    uint32_t* counter;          // batched: zeroed region counter (regions claimed one at a time)
 };
 
 // ---------------------------------------------------------------- decoder ---

@@ -84,12 +84,16 @@ __global__ void __launch_bounds__(kHistThreads, 4)
 }
 
 // Histogram pass of the encoder: the same lane-replicated counters, over the
-// regions of one or many jobs (a contiguous run of regions per CTA).  After
-// each region the CTA folds its 32 copies and stores the difference to the
-// previous fold as that region's histogram, so the encoder can compute every
-// region's bit count without reading its bytes again.  A job's histogram is
-// the sum of its regions', added with one atomic per bin whenever the CTA's
-// run leaves the job.
+// regions of one or many jobs.  After each region the CTA folds its 32 copies
+// and stores the difference to the previous fold as that region's histogram,
+// so the encoder can compute every region's bit count without reading its
+// bytes again.  A job's histogram is the sum of its regions'.  One job (equal
+// regions): each CTA takes a contiguous run of regions and adds the job's sum
+// with one atomic per bin at the end.  Many jobs (a.counter set): regions of
+// very different sizes (a 4 KiB buffer is one region, a 4 MiB one sixteen of
+// 256 KiB), so equal-count runs would leave some CTAs several times the bytes
+// of others; each CTA claims its next region from the counter while it
+// counts the current one, and adds every region's histogram to its job's.
 __global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const __grid_constant__ HistStArgs a) {
     __shared__ uint32_t h[256 * 32];
     for (int i = threadIdx.x; i < 256 * 32; i += kHistThreads) h[i] = 0;
@@ -98,12 +102,23 @@ __global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const __grid_c
     const uint32_t lane4 = (tid & 31) << 2;
     uint32_t prev = 0, acc = 0;  // running fold of bin `tid` (tid < 256); the job's sum so far
     const uint64_t nitems = a.nitems_dev ? *a.nitems_dev : a.nitems;
-    const uint64_t per = (nitems + gridDim.x - 1) / gridDim.x;
-    const uint64_t it0 = (uint64_t)blockIdx.x * per;
-    const uint64_t it1 = it0 + per < nitems ? it0 + per : nitems;
+    const bool claims = a.counter != nullptr;
+    __shared__ uint32_t s_first, s_next;
+    uint64_t it0 = 0, it1 = 0;
+    if (claims) {
+        if (tid == 0) s_first = atomicAdd(a.counter, 1u);
+        __syncthreads();
+        it0 = s_first;
+        it1 = nitems;
+    } else {
+        const uint64_t per = (nitems + gridDim.x - 1) / gridDim.x;
+        it0 = (uint64_t)blockIdx.x * per;
+        it1 = it0 + per < nitems ? it0 + per : nitems;
+    }
     uint32_t job = 0;
-    for (uint64_t it = it0; it < it1; ++it) {
-        if (a.jobs && (it == it0 || it >= a.item0s[job + 1])) job = find_job(a.item0s, a.count, it);
+    for (uint64_t it = it0; it < it1;) {
+        if (claims && tid == 0) s_next = atomicAdd(a.counter, 1u);  // the next region, claimed early
+        if (a.jobs && (claims || it == it0 || it >= a.item0s[job + 1])) job = find_job(a.item0s, a.count, it);
         const EncJob& J = a.jobs ? a.jobs[job] : a.single;
         const uint64_t v0 = (it - J.item0) * (uint64_t)J.st_bytes;
         const uint64_t v1 = (v0 + J.st_bytes < J.hi) ? v0 + J.st_bytes : J.hi;
@@ -132,7 +147,8 @@ __global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const __grid_c
             }
         }
         __syncthreads();
-        const bool leave = it + 1 == it1 || it + 1 == J.item0 + J.nst;
+        const uint64_t next = claims ? (uint64_t)s_next : it + 1;  // read before the second barrier
+        const bool leave = claims || it + 1 == it1 || it + 1 == J.item0 + J.nst;
         if (tid < 256) {
             uint32_t s = 0;
 #pragma unroll 8
@@ -147,6 +163,7 @@ __global__ void __launch_bounds__(kHistThreads, 4) hist_st_kernel(const __grid_c
             }
         }
         __syncthreads();
+        it = next;
     }
     if (a.tag && blockIdx.x == 0 && tid == 0) {
         a.tag[0] = a.single.hi - a.single.lo;
