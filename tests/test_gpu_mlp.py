@@ -1,6 +1,6 @@
 """The learned tuner on the GPU: its CUDA forward, gradient and Adam kernels
 against the float64 oracle, and what the trained network gains over the
-fixed default launch shape (judged against the exhaustive autotuner)."""
+fixed default launch shape (compared with the exhaustive autotuner)."""
 import numpy as np
 import pytest
 import torch
