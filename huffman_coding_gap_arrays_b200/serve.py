@@ -165,6 +165,7 @@ class _Batch:
     plan: BatchCodec | None = None
     dec_ws: torch.Tensor | None = None
     status_host: torch.Tensor | None = None  # the workspaces' status words, copied after the launches
+    lone: tuple | None = None                # a lone compress request's (request, book, sizes, bits, gaps)
     shape: str = ""                          # its launch shape, for the per-shape statistics
 
 
@@ -289,8 +290,13 @@ class Server:
         # pool per stream, and a batch's blocks taken from one shared pool (freed only
         # after the batch's event has fired) never send a new size to the driver mid-run
         # just because the batch landed on another stream than the last one of that size.
-        plan = ent = None
-        if comp:
+        plan = ent = lone = None
+        if len(comp) == 1 and not dec and comp[0].nbytes > 0:
+            # one compress request alone: the single-buffer path (its histogram pass on the
+            # batch's stream, the codebook on the host from the 1 KiB histogram, the encoder)
+            # costs less host work than a batch plan and five launches
+            lone = self._lone_prepare(comp[0], s)
+        elif comp:
             plan = BatchCodec([r.data.numel() for r in comp], cfg, device=self.device, decompress=False,
                               inputs=[r.data for r in comp])
             ent = torch.empty(plan.entries.numel(), dtype=torch.uint8, pin_memory=True)
@@ -311,7 +317,10 @@ class Server:
         b.status_host = self.status_host[s]
         b.status_host.zero_()
         with torch.cuda.stream(s):
-            if comp:
+            if lone is not None:
+                self._lone_launch(comp[0], lone, s, b)
+                b.status_host[0:1].copy_(lone[0].workspace.view(torch.int32)[0:1], non_blocking=True)
+            elif comp:
                 plan.compress(stream=s)
                 ent.copy_(plan.entries, non_blocking=True)
                 b.status_host[0:1].copy_(plan.enc_ws.view(torch.int32)[0:1], non_blocking=True)
@@ -329,6 +338,28 @@ class Server:
     def _bound(self, reqs) -> int:
         kinds = {r.kind for r in reqs}
         return sum(self.request_bytes(r) for r in reqs) + sum(self._fixed[k] for k in kinds)
+
+    def _lone_prepare(self, r, s):
+        """The encoder's histogram pass for one request on stream s, its codebook
+        on the host, and the stream's buffers (allocated on the current stream)."""
+        enc = codec.Encoder(r.nbytes, self.device)
+        hist = torch.empty(256, dtype=torch.int32, device=self.device)
+        s.wait_stream(self.current)
+        enc.histogram(r.data, out=hist, stream=s)
+        hist_host = torch.empty(256, dtype=torch.int32, pin_memory=True)
+        with torch.cuda.stream(s):
+            hist_host.copy_(hist, non_blocking=True)
+        s.synchronize()
+        book, sizes = codec.Codebook.from_histogram(hist_host)
+        bits = torch.empty(max(sizes.words, 1), dtype=torch.int32, device=self.device)
+        gaps = torch.empty(max(sizes.gap_words, 1), dtype=torch.int32, device=self.device)
+        return enc, hist, book, sizes, bits, gaps
+
+    def _lone_launch(self, r, prep, s, b) -> None:
+        enc, hist, book, sizes, bits, gaps = prep
+        enc.encode(r.data, book, sizes, bits=bits, gaps=gaps, stream=s, check_status=False, prepared=True)
+        b.lone = (r, book, sizes, bits[:sizes.words], gaps[:sizes.gap_words])
+        b.keep.append(prep)
 
     def _single_prepare(self, r):
         """Output and workspace of one request decoded by the single-buffer path."""
@@ -390,7 +421,7 @@ class Server:
     def _retire(self, b: _Batch, now: float) -> None:
         # device status of the batch's launches, copied to pinned memory before its event
         words = b.status_host.tolist()
-        if b.plan is not None:
+        if b.plan is not None or b.lone is not None:
             check(lib().hgap_status_from_word(words[0] & 0xffffffff), "served compress")
         if b.dec_ws is not None:
             check(lib().hgap_status_from_word(words[1] & 0xffffffff), "served decompress")
@@ -413,6 +444,13 @@ class Server:
                 # the traffic's byte statistics, for the next batches' features
                 w = min(1.0, r.nbytes / (64 << 20))
                 self.traffic = ((1 - 0.5 * w) * self.traffic + 0.5 * w * entry_features(e)).astype(np.float32)
+        if b.lone is not None:
+            r, book, sizes, bits, gaps = b.lone
+            r.result = codec.Compressed(book, r.nbytes, sizes, bits, gaps) if self.keep_results else int(sizes.words)
+            lens = book.lengths.astype(np.float64)
+            f = np.array([sizes.bits / r.nbytes, lens.max(), float(np.exp2(-lens[lens > 11]).sum())], np.float32)
+            w = min(1.0, r.nbytes / (64 << 20))
+            self.traffic = ((1 - 0.5 * w) * self.traffic + 0.5 * w * f).astype(np.float32)
         if not self.keep_results:
             for r in b.reqs:
                 if r.kind == "decompress":

@@ -86,21 +86,24 @@ def test_request_bound_covers_real_allocations():
         b.event.synchronize()
         assert 0 < b.reserved <= server._bound(reqs)
         server._retire(b, 0.0)
-    # one decompress request alone takes the single-buffer decoder
-    r = SV.Request(9, 0.0, "decompress", stream=streams[0])
-    torch.cuda.synchronize()
-    b = server._launch([r], 0.0)
-    server.held += b.reserved
-    b.event.synchronize()
-    assert 0 < b.reserved <= server._bound([r])
-    server._retire(b, 0.0)
-    assert torch.equal(r.result, bufs[0])
+    # one request alone takes the single-buffer path (decoder, or histogram pass + encoder)
+    for r in (SV.Request(9, 0.0, "decompress", stream=streams[0]), SV.Request(10, 0.0, "compress", data=bufs[1])):
+        torch.cuda.synchronize()
+        b = server._launch([r], 0.0)
+        server.held += b.reserved
+        b.event.synchronize()
+        assert 0 < b.reserved <= server._bound([r])
+        server._retire(b, 0.0)
+        if r.kind == "decompress":
+            assert torch.equal(r.result, bufs[0])
+        else:
+            assert r.result.to_container() == H.compress(bufs[1]).to_container()
     assert server.held == 0
 
 
 def test_light_load_single_requests():
-    """At a light load most batches hold one request (a lone decompress goes
-    through the single-buffer decoder); every result is still exact."""
+    """At a light load most batches hold one request (a lone request goes
+    through the single-buffer path); every result is still exact."""
     server = SV.Server(keep_results=True)
     stats, reqs = _run(server, 24, 1.0, seed=15, hi=2 << 20)
     assert stats["batches"] >= 12
