@@ -241,6 +241,7 @@ __global__ void __launch_bounds__(kTableThreads) bdec_table_kernel(uint32_t coun
     __shared__ BookScratch s;
     __shared__ __align__(16) uint16_t s1[kT1];
     __shared__ __align__(16) uint16_t s2[kDecT2Cap];
+    __shared__ uint16_t s_end[kT1];  // level-2 offset after each prefix's group (0 for none)
     __shared__ uint32_t s_warp[kTableThreads / 32];
     __shared__ uint32_t s_kraft;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -304,26 +305,42 @@ __global__ void __launch_bounds__(kTableThreads) bdec_table_kernel(uint32_t coun
             const uint32_t total = __shfl_sync(kFull, wt, kTableThreads / 32 - 1);
             uint32_t off = (warp ? __shfl_sync(kFull, wt, warp - 1) : 0u) + incl - span;
             if (total <= (uint32_t)kDecT2Cap) {  // uniform; larger only for an incomplete book
-                // pass 2: the pointer prefixes and their level-2 groups
+                // pass 2: the pointer prefixes, and every prefix's level-2 end offset
                 i_first = i_start;
                 for (uint32_t k = 0; k < kPer; ++k) {
                     const uint32_t x = x0 + k;
                     const uint32_t v = x << X;
                     i_first = advance(i_first, v);
-                    if (!(pmask >> k & 1u)) continue;
-                    i_last = advance(i_first, v | ((1u << X) - 1));
-                    const uint32_t w = s.clen[i_last] - P;
-                    s1[x] = (uint16_t)(0x8000u | (w << 12) | off);
-                    uint32_t i = i_first;
-                    for (uint32_t y = 0; y < (1u << w); ++y) {
-                        const uint32_t vy = v | (y << (X - w));
-                        i = advance(i, vy);
-                        s2[off + y] = entry(i, vy);
+                    if (pmask >> k & 1u) {
+                        i_last = advance(i_first, v | ((1u << X) - 1));
+                        const uint32_t w = s.clen[i_last] - P;
+                        s1[x] = (uint16_t)(0x8000u | (w << 12) | off);
+                        off += 1u << w;
                     }
-                    off += 1u << w;
+                    s_end[x] = (uint16_t)off;
                 }
+                __syncthreads();
+                // the level-2 entries, spread over all threads (the pointer prefixes sit
+                // together at the top of the code space, so per-prefix ownership would leave
+                // a few threads with hundreds of entries): entry k belongs to the first prefix
+                // whose end offset exceeds k
                 const uint32_t used = (total + 7) & ~7u;  // whole 16-byte groups, the tail invalid
-                for (uint32_t k = total + tid; k < used; k += kTableThreads) s2[k] = kDecInvalid;
+                for (uint32_t k = tid; k < used; k += kTableThreads) {
+                    uint16_t e2 = kDecInvalid;
+                    if (k < total) {
+                        uint32_t lo = 0, hi = kT1 - 1;
+                        while (lo < hi) {
+                            const uint32_t mid = (lo + hi) >> 1;
+                            if (s_end[mid] > k) hi = mid;
+                            else lo = mid + 1;
+                        }
+                        const uint32_t e1 = s1[lo];  // a pointer entry: width and start of its group
+                        const uint32_t w = (e1 >> 12) & 7u;
+                        const uint32_t vy = (lo << X) | ((k - (e1 & 0xfffu)) << (X - w));
+                        e2 = entry(search(vy), vy);
+                    }
+                    s2[k] = e2;
+                }
                 __syncthreads();
                 c = class_of(s.clen[0], kraft == (1u << kMaxLen));
                 const bool multi = dec_multi(kStageRows[c >> 1], (c & 1u) != 0);
