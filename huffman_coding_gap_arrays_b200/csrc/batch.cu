@@ -16,9 +16,10 @@
 //                   table in shared memory, writes it in the widened form the
 //                   decode kernel keeps in shared memory (DecTableW), and puts
 //                   the buffer in one of 8 classes (decoder stage size by the
-//                   shortest code x complete book or not);
-//   2. bdec_setup   one CTA: tiles per buffer, look-back record numbering,
-//                   and per class the numbering of the class's tiles;
+//                   shortest code x complete book or not), and writes its
+//                   decode job (stream, output, tile count);
+//   2. bdec_setup   one CTA: look-back record numbering over all tiles, and
+//                   per class the numbering of the class's tiles;
 //   3. bdec_map     tile -> buffer map of each class;
 //   4. decode       one persistent launch per class (all 8, or those the
 //                   caller names in dec_class_mask), the single-buffer
@@ -226,7 +227,8 @@ constexpr int kTableThreads = 256;
 
 // One CTA per buffer: checks the entry, builds its two-level decoder table in
 // shared memory and writes the widened form the decode kernel copies per tile
-// (DecTableW), then classifies the buffer.  The table is the one
+// (DecTableW), then classifies the buffer and writes its decode job (all but
+// its first look-back record, which bdec_setup numbers).  The table is the one
 // warp_dec_table builds (book.cuh) -- every level-1 prefix, and every level-2
 // suffix of a prefix whose codes are longer than kDecPrefix bits, takes the
 // symbol whose left-aligned code is the largest not above it; the level-2
@@ -234,7 +236,9 @@ constexpr int kTableThreads = 256;
 // and a block scan places the groups, and the widened entries and the level-2
 // groups in use go out with coalesced stores, in one launch.
 __global__ void __launch_bounds__(kTableThreads) bdec_table_kernel(uint32_t count, const hgap_batch_entry* entries,
-                                                                   DecTableW* wtables, uint8_t* cls,
+                                                                   const uint32_t* bits, const uint32_t* gaps,
+                                                                   uint8_t* const* outputs, uint32_t tile_segs,
+                                                                   DecTableW* wtables, uint8_t* cls, DecJob* jobs,
                                                                    uint32_t* status) {
     constexpr uint32_t P = kDecPrefix, X = kMaxLen - kDecPrefix;  // 11, 5
     constexpr uint32_t kT1 = 1u << P, kPer = kT1 / kTableThreads;  // 8 prefixes a thread
@@ -361,42 +365,12 @@ __global__ void __launch_bounds__(kTableThreads) bdec_table_kernel(uint32_t coun
                 c = kNoClass;
             }
             cls[j] = (uint8_t)c;
-        }
-        __syncthreads();  // s, s1, s2 are reused for the next buffer
-    }
-}
-
-__global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count, const hgap_batch_entry* entries,
-                                                                  const uint8_t* cls, const uint32_t* bits,
-                                                                  const uint32_t* gaps, uint8_t* const* outputs,
-                                                                  DecJob* jobs, uint64_t* item0s,
-                                                                  uint64_t* class_nitems, uint64_t tiles_cap,
-                                                                  uint32_t tile_segs, uint32_t class_mask,
-                                                                  uint32_t* status) {
-    __shared__ uint64_t s_warp[32];
-    uint64_t carry = 0, ccarry[kClasses] = {};
-    for (uint32_t base = 0; base < count; base += kScanThreads) {
-        const uint32_t j = base + threadIdx.x;
-        uint64_t nt = 0;
-        uint32_t c = kNoClass;
-        if (j < count) {
-            c = cls[j];
+            // the buffer's decode job (its first look-back record comes from bdec_setup)
+            uint64_t nt = 0;
             if (c != kNoClass) {  // tiles of the class's decoder
                 const uint64_t segs = dec_tile_segs_for(dec_stage_rows(c / 2 == 0 ? 4 : 4 - c / 2), tile_segs);
-                nt = (entries[j].segments + segs - 1) / segs;
+                nt = (e.segments + segs - 1) / segs;
             }
-        }
-        uint64_t total = 0;
-        const uint64_t rec0 = carry + block_excl_scan_u64(nt, &total, s_warp);
-        carry += total;
-        for (uint32_t k = 0; k < kClasses; ++k) {
-            uint64_t tk = 0;
-            const uint64_t i0 = ccarry[k] + block_excl_scan_u64(c == k ? nt : 0, &tk, s_warp);
-            if (j < count) item0s[(uint64_t)k * (count + 1) + j] = i0;
-            ccarry[k] += tk;
-        }
-        if (j < count) {
-            const hgap_batch_entry& e = entries[j];
             DecJob J;
             memset(&J, 0, sizeof(J));
             J.bits = bits + e.bits_offset;
@@ -408,10 +382,39 @@ __global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count
             J.out_lo = reinterpret_cast<uintptr_t>(out) & 15;
             J.out_aligned = out - J.out_lo;
             J.n = e.n;
-            J.item0 = rec0;
             J.ntiles = nt;
             jobs[j] = J;
         }
+        __syncthreads();  // s, s1, s2 are reused for the next buffer
+    }
+}
+
+// One CTA: the look-back record numbering over all buffers' tiles, and per
+// class the numbering of the class's tiles (the jobs come from bdec_table).
+__global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count, const uint8_t* cls, DecJob* jobs,
+                                                                  uint64_t* item0s, uint64_t* class_nitems,
+                                                                  uint64_t tiles_cap, uint32_t class_mask,
+                                                                  uint32_t* status) {
+    __shared__ uint64_t s_warp[32];
+    uint64_t carry = 0, ccarry[kClasses] = {};
+    for (uint32_t base = 0; base < count; base += kScanThreads) {
+        const uint32_t j = base + threadIdx.x;
+        uint64_t nt = 0;
+        uint32_t c = kNoClass;
+        if (j < count) {
+            c = cls[j];
+            nt = jobs[j].ntiles;  // 0 for a buffer in no class
+        }
+        uint64_t total = 0;
+        const uint64_t rec0 = carry + block_excl_scan_u64(nt, &total, s_warp);
+        carry += total;
+        for (uint32_t k = 0; k < kClasses; ++k) {
+            uint64_t tk = 0;
+            const uint64_t i0 = ccarry[k] + block_excl_scan_u64(c == k ? nt : 0, &tk, s_warp);
+            if (j < count) item0s[(uint64_t)k * (count + 1) + j] = i0;
+            ccarry[k] += tk;
+        }
+        if (j < count) jobs[j].item0 = rec0;
     }
     // a workspace smaller than the query asked for: nothing is decoded
     const bool fits = carry <= tiles_cap;
@@ -698,11 +701,11 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     uint32_t* job_of = reinterpret_cast<uint32_t*>(ws + L.job_of);
 
     if (cudaMemsetAsync(ws, 0, 1024, st) != cudaSuccess) return HGAP_ERR_CUDA;
-    bdec_table_kernel<<<widen_grid(count), kTableThreads, 0, st>>>(count, d_entries, wtables, cls, status);
+    bdec_table_kernel<<<widen_grid(count), kTableThreads, 0, st>>>(count, d_entries, d_bits, d_gaps, d_outputs,
+                                                                   cfg->dec_tile_segs, wtables, cls, jobs, status);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
-    bdec_setup_kernel<<<1, kScanThreads, 0, st>>>(count, d_entries, cls, d_bits, d_gaps, d_outputs, jobs, item0s,
-                                                  class_nitems, L.tiles_cap, cfg->dec_tile_segs, cfg->dec_class_mask,
-                                                  status);
+    bdec_setup_kernel<<<1, kScanThreads, 0, st>>>(count, cls, jobs, item0s, class_nitems, L.tiles_cap,
+                                                  cfg->dec_class_mask, status);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
     bdec_map_kernel<<<book_grid(count), 32 * kBookWarps, 0, st>>>(count, jobs, cls, item0s, job_of, L.tiles_cap);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
