@@ -116,7 +116,9 @@ inline uint64_t encode_super_tiles(uint64_t lo_plus_n, uint64_t n) {
 // the batched ones keep an array of them in the workspace.  Regions (units of
 // st_bytes input bytes) are numbered globally over the jobs of a launch: job
 // j owns regions [item0, item0 + nst).
-struct EncJob {
+// 16-byte aligned (and a multiple of 16 bytes): the one-CTA setup kernels write
+// whole jobs with vector stores
+struct alignas(16) EncJob {
     const uint8_t* in_aligned;  // input rounded down to 16 bytes
     uint64_t lo;                // virtual index of the first input byte (in & 15)
     uint64_t hi;                // lo + n
@@ -133,6 +135,7 @@ struct EncJob {
                                 // part of a stream split across devices (bits / gaps then
                                 // address stream word / gap word 0 of a window)
 };
+static_assert(sizeof(EncJob) == 96, "EncJob: six 16-byte groups");
 
 struct EncArgs {
     EncJob single;              // the job, when jobs == nullptr
@@ -216,7 +219,7 @@ static_assert(sizeof(DecTableW) % 16 == 0, "16-byte copies");
 
 // One stream to decode (same single / batched scheme as EncJob).  Its tiles
 // use look-back records [item0, item0 + ntiles).
-struct DecJob {
+struct alignas(16) DecJob {
     const uint32_t* bits;
     uint64_t words;
     const uint32_t* gaps;
@@ -228,6 +231,7 @@ struct DecJob {
     uint64_t item0;        // first look-back record of the job
     uint64_t ntiles;
 };
+static_assert(sizeof(DecJob) == 80, "DecJob: five 16-byte groups");
 
 struct DecArgs {
     DecJob single;              // the job, when jobs == nullptr
