@@ -537,6 +537,9 @@ def run_serving(args, pool, learned, fixed_cfg, dev):
                     "service = launch to completion"}
     policies = [("autotuner_fixed", dict(config=fixed_cfg))]
     if learned is not None and learned.usable:
+        # the network departs from the shape the search found for the workload only where
+        # it predicts a batch gains more than its margin from another one
+        learned.set_default(fixed_cfg)
         policies.insert(0, ("mlp", dict(tuner=learned)))
     policies.append(("plain", dict(policy="plain")))
     warm = min(5000, max(100, args.serve_requests // 5))

@@ -171,6 +171,12 @@ class LearnedTuner:
         t.holdout_rmse = float(np.sqrt(np.mean((P[ok] - Th[ok]) ** 2))) if ok.any() else float("inf")
         return t
 
+    def set_default(self, cfg: LaunchConfig) -> None:
+        """The shape kept unless a candidate is predicted faster by the margin
+        (e.g. the exhaustive search's pick for the workload); forgets the memo."""
+        self.default = cfg
+        self._memo.clear()
+
     def predict(self, X) -> np.ndarray:
         return np.mean([m.predict(X) for m in self.mlps], axis=0)
 

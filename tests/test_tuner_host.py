@@ -28,3 +28,15 @@ def test_precompute_equals_choose():
         for key, cfg in memo.items():
             t._memo.clear()
             assert t.choose(np.array(key, np.float32)) == cfg, key
+
+
+def test_set_default_forgets_the_memo():
+    from huffman_coding_gap_arrays_b200.batch import LaunchConfig
+    t = M.LearnedTuner([_LinearNet(s) for s in (1, 2)], margin=0.99, dec_margin=0.99)
+    t.precompute(np.array([5.0, 13.0, 0.0], np.float32), 20.0, 21.0, 0.0)
+    assert t._memo
+    fixed = LaunchConfig(region_chunks=32, hist_ctas_per_sm=4, enc_ctas_per_sm=2)
+    t.set_default(fixed)
+    assert not t._memo
+    # no candidate can beat a 99 % margin: the new default is kept
+    assert t.choose(np.array([20.0, 5.0, 13.0, 0.0, 0.0], np.float32)) == fixed
