@@ -175,11 +175,15 @@ class Server:
     def __init__(self, policy: str = "batched", tuner=None, config: LaunchConfig | None = None,
                  hbm_budget: float = 40e9, max_batch: int = 64, max_inflight: int = 3,
                  traffic_features=(5.0, 12.0, 0.05), device="cuda", keep_results: bool = False,
-                 reserve_bytes: int = 8 << 30):
+                 reserve_bytes: int = 8 << 30, tuner_min_bytes: int = 64 << 20):
         if policy not in ("batched", "plain"):
             raise ValueError("policy is 'batched' or 'plain'")
         self.policy = policy
         self.tuner = tuner
+        # below this many bytes a batch's kernels are a small part of its service time (host
+        # work dominates), and shapes the tuner predicts faster on the GPU measured slower in
+        # service: such batches keep the tuner's default shape
+        self.tuner_min_bytes = int(tuner_min_bytes)
         self.config = config or LaunchConfig()
         self.budget = float(hbm_budget)
         self.max_batch = int(max_batch)
@@ -265,6 +269,8 @@ class Server:
     def _config_for(self, reqs) -> LaunchConfig:
         if self.tuner is None:
             return self.config
+        if sum(r.nbytes for r in reqs) < self.tuner_min_bytes:
+            return getattr(self.tuner, "default", self.config)
         f = self._features(reqs)
         memo = getattr(self.tuner, "_memo", None)
         if memo is not None and tuple((np.round(f * 8) / 8).astype(np.float32).tolist()) not in memo:

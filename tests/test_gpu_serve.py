@@ -119,7 +119,7 @@ def test_learned_tuner_policy_and_fixed_shape_agree():
         def choose(self, f):
             return B.LaunchConfig(region_chunks=2, enc_ctas_per_sm=1, dec_ctas_per_sm=2)
 
-    for srv in (SV.Server(keep_results=True, tuner=Fixed()), SV.Server(keep_results=True)):
+    for srv in (SV.Server(keep_results=True, tuner=Fixed(), tuner_min_bytes=0), SV.Server(keep_results=True)):
         reqs = SV.poisson_requests(30, 100.0, pool, streams, seed=13)
         srv.run(reqs)
         _check(reqs, originals)
