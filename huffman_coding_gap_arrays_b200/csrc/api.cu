@@ -198,6 +198,19 @@ hgap_status encode_impl(const void* d_in, uint64_t n, const hgap_codebook* cb, u
     return cuda_status(hgap::launch_encode(a, t, 0, stream));
 }
 
+// The decoder table of the last symbol list this host thread decoded with: a
+// stream is often decoded again with the same book (a served payload, a
+// benchmark loop), and building the table is most of a call's host time.
+struct DecBookCache {
+    bool valid = false;
+    uint32_t count = 0;
+    hgap_symlen symbols[256];
+    uint32_t min_len = 0;
+    bool complete = false;
+    bool pairs = false;
+    hgap::DecTable table;
+};
+
 hgap_status decode_impl(const uint32_t* d_bits, uint64_t words, const uint32_t* d_gaps, uint64_t segments,
                         const hgap_codebook* cb, uint8_t* d_out, uint64_t n, void* d_workspace,
                         size_t workspace_bytes, hgap_stream_t stream, const hgap::LookbackHook& hook) {
@@ -207,15 +220,26 @@ hgap_status decode_impl(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     if (!aligned(d_bits, 4) || !aligned(d_gaps, 4) || !aligned(d_workspace, 8))
         return HGAP_ERR_INVALID_ARG;
     if (words == 0 || segments != (words + 3) / 4) return HGAP_ERR_SIZE;
+    thread_local DecBookCache cache;
+    const bool hit = cache.valid && cb->symbol_count == cache.count &&
+                     std::memcmp(cb->symbols, cache.symbols, sizeof(hgap_symlen) * cache.count) == 0;
     hgap_codebook book;
-    hgap_status s = canonical_copy(cb, &book);
-    if (s != HGAP_OK) return s;
-    if (book.symbol_count == 0) return HGAP_ERR_CORRUPT;
+    hgap_status s = HGAP_OK;
     uint32_t min_len = hgap::kMaxLen;
-    uint64_t kraft = 0;  // units of 2^-16; a complete book (sum 1) has no invalid table entry
-    for (uint32_t i = 0; i < book.symbol_count; ++i) {
-        if (book.symbols[i].length < min_len) min_len = book.symbols[i].length;
-        kraft += 1ull << (hgap::kMaxLen - book.symbols[i].length);
+    bool complete = false;
+    if (hit) {
+        min_len = cache.min_len;
+        complete = cache.complete;
+    } else {
+        s = canonical_copy(cb, &book);
+        if (s != HGAP_OK) return s;
+        if (book.symbol_count == 0) return HGAP_ERR_CORRUPT;
+        uint64_t kraft = 0;  // units of 2^-16; a complete book (sum 1) has no invalid table entry
+        for (uint32_t i = 0; i < book.symbol_count; ++i) {
+            if (book.symbols[i].length < min_len) min_len = book.symbols[i].length;
+            kraft += 1ull << (hgap::kMaxLen - book.symbols[i].length);
+        }
+        complete = kraft == (1ull << hgap::kMaxLen);
     }
     hgap::DecArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -243,14 +267,21 @@ hgap_status decode_impl(const uint32_t* d_bits, uint64_t words, const uint32_t* 
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     // the workspace is cleared on the device while the host builds the table
     if (cudaMemsetAsync(ws, 0, need, st) != cudaSuccess) return HGAP_ERR_CUDA;
-    hgap::DecTable t;
-    s = hgap::make_dec_table(book, &t);
-    if (s != HGAP_OK) return s;
-    const bool complete = kraft == (1ull << hgap::kMaxLen);
-    // two symbols per lookup pay off once about a third of the lookups yield two
-    const bool pairs = hgap::dec_pair_fraction(t) >= 0.3;
+    if (!hit) {
+        cache.valid = false;
+        s = hgap::make_dec_table(book, &cache.table);
+        if (s != HGAP_OK) return s;
+        // two symbols per lookup pay off once about a third of the lookups yield two
+        cache.pairs = hgap::dec_pair_fraction(cache.table) >= 0.3;
+        cache.count = cb->symbol_count;
+        std::memcpy(cache.symbols, cb->symbols, sizeof(hgap_symlen) * cache.count);
+        cache.min_len = min_len;
+        cache.complete = complete;
+        cache.valid = true;
+    }
     a.hook = hook;
-    return cuda_status(hgap::launch_decode(a, t, min_len, complete, pairs, 0, 0, stream));
+    // the table travels as a kernel parameter: copied at launch, so the cache may change after
+    return cuda_status(hgap::launch_decode(a, cache.table, min_len, complete, cache.pairs, 0, 0, stream));
 }
 
 hgap::LookbackHook hold_hook(uint64_t hold, uint64_t wait_limit_ns) {
