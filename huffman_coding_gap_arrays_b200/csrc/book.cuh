@@ -34,9 +34,16 @@
 
 namespace hgap {
 
+// The package-merge lanes read items 16 apart (weights) and about 8 apart
+// (leaves): unpadded, a whole warp's 8-byte reads land in one bank pair (the
+// capture of one-warp-per-book showed two thirds of its shared wavefronts were
+// conflicts).  One pad slot per 16 weights and per 8 keys spreads them.
+__device__ __forceinline__ uint32_t wpad(uint32_t i) { return i + (i >> 4); }
+__device__ __forceinline__ uint32_t kpad(uint32_t i) { return i + (i >> 3); }
+
 struct BookScratch {
-    uint64_t w[2][512];           // weights of two consecutive package-merge levels
-    uint64_t key[256];            // count << 8 | byte, ~0 for absent bytes; sorted in place
+    uint64_t w[2][512 + 32];      // weights of two consecutive package-merge levels (at wpad)
+    uint64_t key[256 + 32];       // count << 8 | byte, ~0 for absent bytes; sorted in place (at kpad)
     uint16_t pk[kMaxLen + 1][32]; // bit b of pk[l][q]: item 16q+b of level l is a package
     uint16_t size[kMaxLen + 1];   // items kept at each level
     uint32_t la[256];             // container order: code << (16 - length)
@@ -53,14 +60,14 @@ __device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t lane, ui
 }
 
 // Fills s.key (sorted) and s.len for the present bytes of `hist` and returns
-// their number n.  Leaf r (ascending count, ties by byte) is s.key[r].
+// their number n.  Leaf r (ascending count, ties by byte) is s.key[kpad(r)].
 __device__ inline uint32_t warp_code_lengths(const uint32_t* hist, BookScratch& s, uint32_t lane) {
     uint32_t n = 0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const uint32_t b = lane + 32 * j;
         const uint32_t h = hist[b];
-        s.key[b] = h ? (((uint64_t)h << 8) | b) : ~0ull;
+        s.key[kpad(b)] = h ? (((uint64_t)h << 8) | b) : ~0ull;
         n += __popc(__ballot_sync(kFull, h != 0));
     }
     __syncwarp();
@@ -71,10 +78,10 @@ __device__ inline uint32_t warp_code_lengths(const uint32_t* hist, BookScratch& 
             for (uint32_t t = lane; t < 128; t += 32) {
                 const uint32_t i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
                 const uint32_t p = i + j;
-                const uint64_t x = s.key[i], y = s.key[p];
+                const uint64_t x = s.key[kpad(i)], y = s.key[kpad(p)];
                 if ((x > y) == ((i & k) == 0)) {
-                    s.key[i] = y;
-                    s.key[p] = x;
+                    s.key[kpad(i)] = y;
+                    s.key[kpad(p)] = x;
                 }
             }
             __syncwarp();
@@ -88,7 +95,7 @@ __device__ inline uint32_t warp_code_lengths(const uint32_t* hist, BookScratch& 
     if (n < 2) return n;
 
     const uint32_t keep = 2 * n - 2;
-    for (uint32_t r = lane; r < 512; r += 32) s.w[0][r] = r < n ? (s.key[r] >> 8) : 0;
+    for (uint32_t r = lane; r < 512; r += 32) s.w[0][wpad(r)] = r < n ? (s.key[kpad(r)] >> 8) : 0;
     s.pk[1][lane] = 0;
     if (lane == 0) s.size[1] = (uint16_t)n;
     __syncwarp();
@@ -107,19 +114,19 @@ __device__ inline uint32_t warp_code_lengths(const uint32_t* hist, BookScratch& 
             while (lo < hi) {
                 const uint32_t mid = (lo + hi) >> 1;
                 const uint32_t jj = d - mid - 1;
-                if ((s.key[mid] >> 8) < below[2 * jj] + below[2 * jj + 1]) lo = mid + 1;
+                if ((s.key[kpad(mid)] >> 8) < below[wpad(2 * jj)] + below[wpad(2 * jj + 1)]) lo = mid + 1;
                 else hi = mid;
             }
             uint32_t i = lo, j = d - lo;
             const uint32_t e = d + 16 < m ? d + 16 : m;
             for (uint32_t pos = d; pos < e; ++pos) {
-                const uint64_t pw = j < np ? below[2 * j] + below[2 * j + 1] : 0;
-                if (j < np && (i >= n || pw <= (s.key[i] >> 8))) {
-                    out[pos] = pw;
+                const uint64_t pw = j < np ? below[wpad(2 * j)] + below[wpad(2 * j + 1)] : 0;
+                if (j < np && (i >= n || pw <= (s.key[kpad(i)] >> 8))) {
+                    out[wpad(pos)] = pw;
                     mask |= 1u << (pos - d);
                     ++j;
                 } else {
-                    out[pos] = s.key[i] >> 8;
+                    out[wpad(pos)] = s.key[kpad(i)] >> 8;
                     ++i;
                 }
             }
@@ -168,7 +175,7 @@ __device__ inline uint32_t warp_assign_codes(BookScratch& s, uint32_t n, uint32_
         if (c < n) {
             const uint32_t r = n - 1 - c;
             const uint32_t L = s.len[r];
-            const uint32_t sym = (uint32_t)(s.key[r] & 0xff);
+            const uint32_t sym = (uint32_t)(s.key[kpad(r)] & 0xff);
             s.sym[c] = (uint8_t)sym;
             s.clen[c] = (uint8_t)L;
             s.blen[sym] = (uint8_t)L;
