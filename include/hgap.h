@@ -216,10 +216,9 @@ hgap_status hgap_decode_hold(const uint32_t* d_bits, uint64_t words, const uint3
  * with hgap_decode_workspace_bytes(segments) > HGAP_NOALLOC_SCRATCH_BYTES are
  * rejected with HGAP_ERR_WORKSPACE before anything runs.  The call waits for
  * `stream` and returns the device-side status too.  The first call on each
- * device looks up the array's device address; make it before any stream
- * capture.  The address is kept for the life of the process, so a
- * cudaDeviceReset between calls (which unloads the library's device code and
- * may move the array) is not supported.  All calls share the one array: calls
+ * device looks up the array's device address, which is kept for the life of
+ * the process, so a cudaDeviceReset between calls (which unloads the
+ * library's device code and may move the array) is not supported.  All calls share the one array: calls
  * that overlap on the GPU (other streams, other host threads) race and must
  * be serialized by the caller.  Allocates nothing. */
 #define HGAP_NOALLOC_SCRATCH_BYTES (256u * 1024u)
