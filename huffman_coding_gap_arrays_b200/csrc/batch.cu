@@ -234,8 +234,10 @@ constexpr int kTableThreads = 256;
 // symbol whose left-aligned code is the largest not above it; the level-2
 // groups sit in prefix order -- but every thread owns 8 consecutive prefixes
 // and a block scan places the groups, and the widened entries and the level-2
-// groups in use go out with coalesced stores, in one launch.
-__global__ void __launch_bounds__(kTableThreads) bdec_table_kernel(uint32_t count, const hgap_batch_entry* entries,
+// groups in use go out with coalesced stores, in one launch.  At 32 registers
+// a thread (no spills) seven CTAs fit an SM, bound by shared memory, where 40
+// registers allowed six.
+__global__ void __launch_bounds__(kTableThreads, 8) bdec_table_kernel(uint32_t count, const hgap_batch_entry* entries,
                                                                    const uint32_t* bits, const uint32_t* gaps,
                                                                    uint8_t* const* outputs, uint32_t tile_segs,
                                                                    DecTableW* wtables, uint8_t* cls, DecJob* jobs,
@@ -391,39 +393,83 @@ __global__ void __launch_bounds__(kTableThreads) bdec_table_kernel(uint32_t coun
 
 // One CTA: the look-back record numbering over all buffers' tiles, and per
 // class the numbering of the class's tiles (the jobs come from bdec_table).
+// Per 1024 buffers: nine warp scans of the tile counts (all tiles, and one per
+// class with the other classes' buffers counting 0) need no barrier; nine
+// warps then scan the 32 warp totals of one sum each, between two barriers,
+// and every buffer writes its record and, for its own class only, its first
+// class tile (the only entry the map and the decoder read).  The next 1024
+// buffers' loads are in flight meanwhile.
 __global__ void __launch_bounds__(kScanThreads) bdec_setup_kernel(uint32_t count, const uint8_t* cls, DecJob* jobs,
                                                                   uint64_t* item0s, uint64_t* class_nitems,
                                                                   uint64_t tiles_cap, uint32_t class_mask,
                                                                   uint32_t* status) {
-    __shared__ uint64_t s_warp[32];
-    uint64_t carry = 0, ccarry[kClasses] = {};
-    for (uint32_t base = 0; base < count; base += kScanThreads) {
-        const uint32_t j = base + threadIdx.x;
-        uint64_t nt = 0;
-        uint32_t c = kNoClass;
-        if (j < count) {
-            c = cls[j];
-            nt = jobs[j].ntiles;  // 0 for a buffer in no class
-        }
-        uint64_t total = 0;
-        const uint64_t rec0 = carry + block_excl_scan_u64(nt, &total, s_warp);
-        carry += total;
-        for (uint32_t k = 0; k < kClasses; ++k) {
-            uint64_t tk = 0;
-            const uint64_t i0 = ccarry[k] + block_excl_scan_u64(c == k ? nt : 0, &tk, s_warp);
-            if (j < count) item0s[(uint64_t)k * (count + 1) + j] = i0;
-            ccarry[k] += tk;
-        }
-        if (j < count) jobs[j].item0 = rec0;
+    constexpr uint32_t kSums = kClasses + 1;  // the classes, then all tiles
+    constexpr uint32_t kWarps = kScanThreads / 32;
+    __shared__ uint64_t s_tot[2][kSums][kWarps];  // by chunk parity: warp totals, then warp offsets
+    __shared__ uint64_t s_carry[kSums];           // the sums over the earlier chunks
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x < kSums) s_carry[threadIdx.x] = 0;
+    uint32_t c_next = kNoClass;
+    uint64_t nt_next = 0;
+    if (threadIdx.x < count) {
+        c_next = cls[threadIdx.x];
+        nt_next = jobs[threadIdx.x].ntiles;  // 0 for a buffer in no class
     }
+    uint32_t par = 0;
+    for (uint64_t base = 0; base < count; base += kScanThreads, par ^= 1u) {
+        const uint64_t j = base + threadIdx.x;
+        const uint32_t c = c_next;
+        const uint64_t nt = nt_next;
+        const uint64_t jn = j + kScanThreads;
+        c_next = kNoClass;
+        nt_next = 0;
+        if (jn < count) {
+            c_next = cls[jn];
+            nt_next = jobs[jn].ntiles;
+        }
+        uint64_t x_all = nt, x_own = 0;
+        for (uint32_t k = 0; k < kSums; ++k) {
+            uint64_t x = k == kClasses ? nt : (c == k ? nt : 0);
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint64_t t = __shfl_up_sync(kFull, x, d);
+                if (lane >= (uint32_t)d) x += t;
+            }
+            if (lane == 31) s_tot[par][k][warp] = x;
+            if (k == kClasses) x_all = x;
+            else if (c == k) x_own = x;
+        }
+        __syncthreads();
+        if (warp < kSums) {
+            const uint64_t v = s_tot[par][warp][lane];
+            uint64_t x = v;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint64_t t = __shfl_up_sync(kFull, x, d);
+                if (lane >= (uint32_t)d) x += t;
+            }
+            const uint64_t carry = s_carry[warp];
+            __syncwarp();
+            s_tot[par][warp][lane] = carry + x - v;
+            if (lane == 31) s_carry[warp] = carry + x;
+        }
+        __syncthreads();
+        if (j < count) {
+            jobs[j].item0 = s_tot[par][kClasses][warp] + x_all - nt;
+            if (c < kClasses) item0s[(uint64_t)c * (count + 1) + j] = s_tot[par][c][warp] + x_own - nt;
+        }
+    }
+    // (the last chunk's second barrier orders every s_carry update before these reads)
+    const uint64_t all = s_carry[kClasses];
     // a workspace smaller than the query asked for: nothing is decoded
-    const bool fits = carry <= tiles_cap;
+    const bool fits = all <= tiles_cap;
     if (threadIdx.x == 0 && !fits) atomicOr(status, kDevSize);
     if (threadIdx.x < kClasses) {
-        item0s[(uint64_t)threadIdx.x * (count + 1) + count] = ccarry[threadIdx.x];
-        class_nitems[threadIdx.x] = fits ? ccarry[threadIdx.x] : 0;
+        const uint64_t tk = s_carry[threadIdx.x];
+        item0s[(uint64_t)threadIdx.x * (count + 1) + count] = tk;
+        class_nitems[threadIdx.x] = fits ? tk : 0;
         // a class the caller left out of the launch holds buffers: they stay undecoded
-        if (class_mask && ccarry[threadIdx.x] && !(class_mask >> threadIdx.x & 1u)) atomicOr(status, kDevPlan);
+        if (class_mask && tk && !(class_mask >> threadIdx.x & 1u)) atomicOr(status, kDevPlan);
     }
 }
 
@@ -476,9 +522,12 @@ unsigned book_grid(uint32_t count) {
     return (unsigned)(want < cap ? (want ? want : 1) : cap);
 }
 
-unsigned widen_grid(uint32_t count) {
-    const uint64_t cap = (uint64_t)sm_count() * 8;
-    return (unsigned)(count < cap ? (count ? count : 1) : cap);
+// One CTA per buffer: the block scheduler hands a buffer to whichever SM frees
+// a slot first, where a grid of a fixed multiple of the SMs that looped over
+// the buffers started its last CTAs only after the first ones' loops ended.
+unsigned table_grid(uint32_t count) {
+    constexpr uint32_t kMax = 1u << 24;
+    return count < kMax ? (count ? count : 1) : kMax;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -701,7 +750,7 @@ hgap_status hgap_batch_decompress(uint32_t count, const hgap_batch_entry* d_entr
     uint32_t* job_of = reinterpret_cast<uint32_t*>(ws + L.job_of);
 
     if (cudaMemsetAsync(ws, 0, 1024, st) != cudaSuccess) return HGAP_ERR_CUDA;
-    bdec_table_kernel<<<widen_grid(count), kTableThreads, 0, st>>>(count, d_entries, d_bits, d_gaps, d_outputs,
+    bdec_table_kernel<<<table_grid(count), kTableThreads, 0, st>>>(count, d_entries, d_bits, d_gaps, d_outputs,
                                                                    cfg->dec_tile_segs, wtables, cls, jobs, status);
     if (cudaGetLastError() != cudaSuccess) return HGAP_ERR_CUDA;
     bdec_setup_kernel<<<1, kScanThreads, 0, st>>>(count, cls, jobs, item0s, class_nitems, L.tiles_cap,
