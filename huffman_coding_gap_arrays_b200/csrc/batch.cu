@@ -37,7 +37,9 @@
 namespace hgap {
 namespace {
 
-constexpr int kBookWarps = 4;
+// Books (warps) per CTA of the book kernels: 14 KiB of scratch a book, so two a
+// CTA put 14 books on an SM (seven CTAs), where four a CTA fitted 12 (three).
+constexpr int kBookWarps = 2;
 constexpr size_t kBookSmem = kBookWarps * sizeof(BookScratch);
 constexpr int kScanThreads = 1024;
 constexpr uint32_t kClasses = 8;
@@ -72,6 +74,42 @@ __device__ __forceinline__ uint64_t block_excl_scan_u64(uint64_t v, uint64_t* to
     return before + x - v;
 }
 
+// The same for two values per thread at once (one set of barriers).
+__device__ __forceinline__ void block_excl_scan2_u64(uint64_t& a, uint64_t& b, uint64_t* total_a, uint64_t* total_b,
+                                                     uint64_t (*s_warp)[32]) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t x = a, y = b;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint64_t t = __shfl_up_sync(kFull, x, d);
+        const uint64_t u = __shfl_up_sync(kFull, y, d);
+        if (lane >= (uint32_t)d) {
+            x += t;
+            y += u;
+        }
+    }
+    if (lane == 31) {
+        s_warp[0][warp] = x;
+        s_warp[1][warp] = y;
+    }
+    __syncthreads();
+    if (warp < 2) {
+        uint64_t w = s_warp[warp][lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint64_t t = __shfl_up_sync(kFull, w, d);
+            if (lane >= (uint32_t)d) w += t;
+        }
+        s_warp[warp][lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    a = (warp ? s_warp[0][warp - 1] : 0) + x - a;
+    b = (warp ? s_warp[1][warp - 1] : 0) + y - b;
+    *total_a = s_warp[0][31];
+    *total_b = s_warp[1][31];
+    __syncthreads();  // s_warp free for the next call
+}
+
 // --------------------------------------------------------------- compress ---
 
 __global__ void __launch_bounds__(kScanThreads) benc_setup_kernel(uint32_t count, const uint8_t* const* inputs,
@@ -82,16 +120,31 @@ __global__ void __launch_bounds__(kScanThreads) benc_setup_kernel(uint32_t count
                                                                   uint64_t max_regions, uint32_t* status) {
     __shared__ uint64_t s_warp[32];
     uint64_t carry = 0;
-    for (uint32_t base = 0; base < count; base += kScanThreads) {
-        const uint32_t j = base + threadIdx.x;
-        uint64_t nst = 0, n = 0, lo = 0;
-        uint32_t st = 0;
-        const uint8_t* in = nullptr;
+    // each buffer's size, input pointer and region size, the next 1024 buffers' in flight
+    uint64_t n_next = 0;
+    const uint8_t* in_next = nullptr;
+    uint32_t rc_next = base_chunks;
+    auto load = [&](uint64_t j) {
+        n_next = 0;
+        in_next = nullptr;
+        rc_next = base_chunks;
         if (j < count) {
-            n = sizes[j];
-            in = inputs[j];
+            n_next = sizes[j];
+            in_next = inputs[j];
+            if (region_chunks) rc_next = region_chunks[j];
+        }
+    };
+    load(threadIdx.x);
+    for (uint64_t base = 0; base < count; base += kScanThreads) {
+        const uint64_t j = base + threadIdx.x;
+        const uint64_t n = n_next;
+        const uint8_t* const in = in_next;
+        uint32_t rc = rc_next;
+        load(j + kScanThreads);
+        uint64_t nst = 0, lo = 0;
+        uint32_t st = 0;
+        if (j < count) {
             lo = reinterpret_cast<uintptr_t>(in) & 15;
-            uint32_t rc = region_chunks ? region_chunks[j] : base_chunks;
             if (rc < base_chunks) rc = base_chunks;
             if (rc > 32) rc = 32;
             st = rc * (uint32_t)kEncChunkBytes;
@@ -176,24 +229,35 @@ __global__ void __launch_bounds__(kScanThreads) benc_place_kernel(uint32_t count
                                                                   EncJob* jobs, uint32_t* bits,
                                                                   uint64_t bits_cap, uint32_t* gaps,
                                                                   uint64_t gaps_cap, uint32_t* status) {
-    __shared__ uint64_t s_warp[32];
+    __shared__ uint64_t s_warp[2][32];
     uint64_t cb = 0, cg = 0;
-    for (uint32_t base = 0; base < count; base += kScanThreads) {
-        const uint32_t j = base + threadIdx.x;
-        uint64_t w = 0, g = 0;
+    // each stream's words, gap words and segments, the next 1024 streams' in flight
+    uint64_t w_next = 0, g_next = 0, s_next = 0;
+    auto load = [&](uint64_t j) {
+        w_next = 0;
+        g_next = 0;
+        s_next = 0;
         if (j < count) {
-            w = (entries[j].words + 3) & ~3ull;
-            g = entries[j].gap_words;
+            w_next = entries[j].words;
+            g_next = entries[j].gap_words;
+            s_next = entries[j].segments;
         }
-        uint64_t tb = 0, tg = 0;
-        const uint64_t ob = cb + block_excl_scan_u64(w, &tb, s_warp);
-        const uint64_t og = cg + block_excl_scan_u64(g, &tg, s_warp);
+    };
+    load(threadIdx.x);
+    for (uint64_t base = 0; base < count; base += kScanThreads) {
+        const uint64_t j = base + threadIdx.x;
+        const uint64_t words = w_next, gap_words = g_next, segments = s_next;
+        load(j + kScanThreads);
+        uint64_t ob = (words + 3) & ~3ull, og = gap_words, tb = 0, tg = 0;
+        block_excl_scan2_u64(ob, og, &tb, &tg, s_warp);
+        ob += cb;
+        og += cg;
         if (j < count) {
             hgap_batch_entry& e = entries[j];
             EncJob& J = jobs[j];
             e.bits_offset = ob;
             e.gaps_offset = og;
-            if (ob + e.words > bits_cap || og + e.gap_words > gaps_cap) {
+            if (ob + words > bits_cap || og + gap_words > gaps_cap) {
                 e.status = HGAP_ERR_SIZE;  // the arena is too small: this stream is not written
                 atomicOr(status, kDevSize);
                 J.bits = bits;
@@ -202,11 +266,11 @@ __global__ void __launch_bounds__(kScanThreads) benc_place_kernel(uint32_t count
                 J.gap_words = 0;
             } else {
                 J.bits = bits + ob;
-                J.words = e.words;
+                J.words = words;
                 J.gaps = gaps + og;
-                J.gap_words = e.gap_words;
+                J.gap_words = gap_words;
             }
-            J.segments = e.segments;
+            J.segments = segments;
             J.bits_aligned16 = 1;
         }
         cb += tb;
@@ -509,16 +573,16 @@ __global__ void __launch_bounds__(32 * kBookWarps) dec_table_kernel(uint32_t cou
 
 // --------------------------------------------------------- host helpers ---
 
-int sm_count() { return current_sm_count(); }
-
 template <class K>
 cudaError_t set_book_smem(K kern) {
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBookSmem);
 }
 
+// One warp per book (or buffer), every CTA launched at once: the block
+// scheduler starts each as a slot frees.
 unsigned book_grid(uint32_t count) {
     const uint64_t want = (count + kBookWarps - 1) / kBookWarps;
-    const uint64_t cap = (uint64_t)sm_count() * 8;
+    const uint64_t cap = 1u << 24;
     return (unsigned)(want < cap ? (want ? want : 1) : cap);
 }
 
