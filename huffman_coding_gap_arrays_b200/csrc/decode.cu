@@ -260,6 +260,14 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R, SEGS>::kMinBlocks)
         const uint4* s1 = reinterpret_cast<const uint4*>(t.t1);
         for (int i = tid; i < C::kT1 / 4; i += kDecThreads) reinterpret_cast<uint4*>(t1)[i] = s1[i];
     };
+    // the same for the next tile of another job, as soon as this tile's decode is
+    // done (nothing reads `t1` again before the next tile): asynchronous copies,
+    // so their L2 round trip overlaps the look-back, write-out and compaction
+    auto copy_tables_async = [&](const DecTableW& t) {
+        const uint4* s1 = reinterpret_cast<const uint4*>(t.t1);
+        for (int i = tid; i < C::kT1 / 4; i += kDecThreads) cp_async16(reinterpret_cast<uint4*>(t1) + i, s1 + i);
+        cp_async_commit();
+    };
     // thread 0: the tile `item` and its job into slot s
     auto fill_slot = [&](int s, uint64_t item) {
         DecSlot& d = slot[s];
@@ -388,6 +396,8 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R, SEGS>::kMinBlocks)
         __syncthreads();  // (2) decode done; next tile known
         const DecSlot& N = slot[ns];
         const bool have_next = N.item < s_nitems;
+        const bool reload = a.jobs && have_next && N.job_id != s_lut_job;
+        if (reload) copy_tables_async(a.tables[N.job_id]);
         const uint32_t wt = warp_incl_scan(lane < (uint32_t)C::kWarps ? warp_tot[lane] : 0u, lane);
         const uint32_t totals = __shfl_sync(kFull, wt, C::kWarps - 1);
         const uint32_t before = warp ? __shfl_sync(kFull, wt, warp - 1) : 0u;
@@ -485,8 +495,8 @@ __global__ void __launch_bounds__(kDecThreads, DecCfg<R, SEGS>::kMinBlocks)
                 if (tl > 2) compact[d + t + 2] = src[t + 2];
             }
         }
-        if (have_next) {  // sg and the tables are no longer read for this tile
-            if (a.jobs && N.job_id != s_lut_job) copy_tables(a.tables[N.job_id]);
+        if (have_next) {  // sg is no longer read for this tile
+            if (reload) cp_async_wait_all();
             if (tid < (uint32_t)C::kGapStage) sg[tid] = pre_gap;
         }
         prev_s = have ? ti : -1;
