@@ -22,9 +22,10 @@ smaller one (zipf_16m) has L2 flushed before every step, outside its timing.
 Prints one JSON line.  `value` = uncompressed bytes of all ranks / (max over
 ranks of the device time of K steps); `e2e` = the same through the public API
 with pinned host buffers and the H2D/D2H copies inside the timed region.
-The path partitions by buffer: with N > 1 the batch's buffers are sharded
-across the ranks by bytes (strong scaling, no collective on the data path);
-`--replicas` gives every rank a whole batch instead (weak scaling).
+The path partitions by buffer, with no collective on the data path: with
+N > 1 every rank compresses and decompresses its own 4096-buffer batch (drawn
+with its own seeds: a job of N x 4096 buffers, weak scaling); `--shard` splits
+the one 4096-buffer batch across the ranks by bytes instead (strong scaling).
 """
 from __future__ import annotations
 
@@ -66,8 +67,9 @@ def parse():
     p.add_argument("--plain-buffers", type=int, default=4096,
                    help="buffers of the batch timed through the plain per-buffer path")
     p.add_argument("--no-tune", action="store_true", help="skip tuning: fixed default launch shape")
-    p.add_argument("--replicas", action="store_true",
-                   help="N > 1: every rank runs its own whole batch (weak scaling) instead of a share of one")
+    p.add_argument("--shard", action="store_true",
+                   help="N > 1: split one batch across the ranks by bytes (strong scaling) instead of "
+                        "giving every rank its own batch (weak scaling)")
     p.add_argument("--serve-requests", type=int, default=100000,
                    help="requests of the serving run (0: none)")
     p.add_argument("--serve-payloads", type=int, default=1024,
@@ -675,7 +677,7 @@ def run_batch(args, rank, world, dev, pg):
     desc = WORKLOADS["batch4096"][0]
     if args.batch_count != 4096:
         desc = desc.replace("4096 uint8 buffers", f"{args.batch_count} uint8 buffers (profiling size)")
-    shard = world > 1 and not args.replicas
+    shard = world > 1 and args.shard
     if shard:  # one batch, each rank its byte-balanced share: no collective on the data path
         all_sizes = WL.batch_sizes(args.batch_count, seed=4)
         mine = PL.shard_by_bytes(all_sizes, world)[rank]
@@ -859,7 +861,8 @@ def run_batch(args, rank, world, dev, pg):
             "dtype": "u8", "data": "synthetic",
             "config": {"workload": desc, "buffers": len(sizes), "bytes_per_gpu": total,
                        "parallelism": (f"batch sharded by bytes over {world} ranks, no data-path collective"
-                                       if shard else f"replicas x{world}"),
+                                       if shard else f"{world} rank(s), each its own batch (own seeds), "
+                                                     "no data-path collective"),
                        "step": "batched compress (device histograms, codebooks, encode) then batched "
                                "decompress, two captured CUDA graphs",
                        "l2": (f"inputs ({total / 1e9:.2f} GB per GPU) larger than the 126 MB L2; no flush"
