@@ -685,7 +685,11 @@ def run_batch(args, rank, world, dev, pg):
         job_bytes = sum(all_sizes)
     else:
         sizes, flat, ins = batch_workload(dev, rank, args.batch_count)
-        job_bytes = world * sum(sizes)
+        job_bytes = sum(sizes)
+        if pg:  # every rank's own batch (its own sizes): the job is all of them, summed once, untimed
+            t = torch.tensor([job_bytes], dtype=torch.int64, device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.SUM)
+            job_bytes = int(t.item())
     total = sum(sizes)
     flat_out = torch.empty(total, dtype=torch.uint8, device=dev)
     outs, p = [], 0
