@@ -127,6 +127,22 @@ def quantize_features(f) -> np.ndarray:
     return np.array([size, ent, maxlen, l2, count], np.float32)
 
 
+def precompute_grid(tuner, sizes, max_batch: int) -> None:
+    """Fills the tuner's memo for every batch a run over requests of `sizes`
+    can form, before the clock starts: all batch sizes from the smallest
+    request to the largest `max_batch` requests together, over the grid of
+    `quantize_features` (byte statistics and log2 of the request count)."""
+    if not len(sizes):
+        return
+    lo = np.log2(max(1, min(sizes)))
+    hi = np.log2(max(1, sum(sorted(sizes)[-max_batch:])))
+    for e in FEATURE_ENTROPY:
+        for m in FEATURE_MAXLEN:
+            for l2 in FEATURE_L2:
+                for k in range(int(np.round(np.log2(max_batch))) + 1):
+                    tuner.precompute(np.array([e, m, l2], np.float32), lo, hi, float(k))
+
+
 ALLOC_GRAIN = 512  # the caching allocator rounds every block up to a multiple of this
 # ...and a block of 1 MiB or more may keep an unsplit remainder of up to 1 MiB
 # (the allocator splits a large block only when more than 1 MiB would be left)
@@ -469,16 +485,7 @@ class Server:
         latency and throughput statistics."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         if self.policy != "plain" and self.tuner is not None and hasattr(self.tuner, "precompute"):
-            # every batch the run can form, decided before the clock starts: all sizes
-            # from the smallest request to the largest batch, over the feature grid
-            sizes = [r.nbytes for r in reqs]
-            lo = np.log2(max(1, min(sizes)))
-            hi = np.log2(max(1, sum(sorted(sizes)[-self.max_batch:])))
-            for e in FEATURE_ENTROPY:
-                for m in FEATURE_MAXLEN:
-                    for l2 in FEATURE_L2:
-                        for k in range(int(np.round(np.log2(self.max_batch))) + 1):
-                            self.tuner.precompute(np.array([e, m, l2], np.float32), lo, hi, float(k))
+            precompute_grid(self.tuner, [r.nbytes for r in reqs], self.max_batch)
         # the cyclic garbage collector stays off while the clock runs: a full pass over
         # the run's objects stalled a launch for ~100 ms and every request queued behind it
         gc_on = gc.isenabled()
@@ -604,4 +611,5 @@ def encode_streams(buffers, config: LaunchConfig | None = None) -> list:
                           plan.gaps[e.gaps_offset:e.gaps_offset + e.gap_words], plan) for e in ents]
 
 
-__all__ = ["Server", "Request", "EncodedStream", "poisson_requests", "encode_streams", "quantize_features"]
+__all__ = ["Server", "Request", "EncodedStream", "poisson_requests", "encode_streams", "quantize_features",
+           "precompute_grid"]

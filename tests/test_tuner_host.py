@@ -40,3 +40,28 @@ def test_set_default_forgets_the_memo():
     assert not t._memo
     # no candidate can beat a 99 % margin: the new default is kept
     assert t.choose(np.array([20.0, 5.0, 13.0, 0.0, 0.0], np.float32)) == fixed
+
+
+def test_serving_batches_hit_the_precomputed_memo():
+    """Every batch a serving run can form -- any 1..max_batch of its requests,
+    any byte statistics -- quantizes to a memo entry the run filled before its
+    clock started, so no batch waits for a forward pass."""
+    from huffman_coding_gap_arrays_b200 import serve as S
+    t = M.LearnedTuner([_LinearNet(s) for s in (4, 5)], margin=0.0, dec_margin=0.0)
+    rng = np.random.default_rng(9)
+    sizes = [int(x) for x in np.exp(rng.uniform(np.log(64 << 10), np.log(64 << 20), 400))]
+    max_batch = 48
+    S.precompute_grid(t, sizes, max_batch)
+    filled = dict(t._memo)
+    assert filled
+    for _ in range(2000):
+        k = int(rng.integers(1, max_batch + 1))
+        pick = rng.choice(len(sizes), size=k, replace=False)
+        nb = np.array([sizes[i] for i in pick], np.float64)
+        stats = np.stack([rng.uniform(0, 8.5, k), rng.uniform(1, 16, k), rng.uniform(0, 1, k) ** 3], axis=1)
+        f = S.quantize_features(np.concatenate([[np.log2(nb.sum())], (nb[:, None] * stats).sum(0) / nb.sum(),
+                                                [np.log2(k)]]))
+        key = tuple((np.round(np.asarray(f, np.float32) * 8) / 8).tolist())
+        assert key in filled, key
+        assert t.choose(f) == filled[key]
+    assert len(t._memo) == len(filled)  # nothing was added: every choice came from the memo
