@@ -193,3 +193,54 @@ def test_batch_decoder_class():
     assert cls([4] * 16) == 1
     assert cls([8] * 256) == 1
     assert cls([5] * 8) == 0
+
+
+def test_container_parse_survives_random_damage():
+    """The container reader on thousands of damaged containers (bytes flipped,
+    cut short, lengthened): it rejects them or accepts a consistent one, whose
+    stream and gap pointers lie inside the buffer and whose book is valid --
+    never a read past the buffer."""
+    L = _lib.lib()
+    rng = np.random.default_rng(21)
+    blobs = []
+    for n, dist in ((5000, "zipf"), (777, "few"), (1, "one")):
+        if dist == "zipf":
+            p = np.arange(1, 257, dtype=np.float64) ** -1.2
+            x = rng.choice(256, size=n, p=p / p.sum()).astype(np.uint8)
+        elif dist == "few":
+            x = rng.integers(0, 5, n).astype(np.uint8)
+        else:
+            x = np.array([42], np.uint8)
+        cb = O.codebook(O.histogram(x))
+        bits, gaps, B = O.encode(x, cb)
+        blobs.append(O.container(cb, x.size, bits, gaps, (B + 127) // 128))
+    accepted = 0
+    for it in range(3000):
+        blob = bytearray(blobs[it % len(blobs)])
+        kind = it % 3
+        if kind == 0:
+            for _ in range(int(rng.integers(1, 4))):
+                blob[int(rng.integers(0, len(blob)))] ^= 1 << int(rng.integers(0, 8))
+        elif kind == 1:
+            blob = blob[:int(rng.integers(0, len(blob)))]
+        else:
+            blob += bytes(rng.integers(0, 256, int(rng.integers(1, 64))).astype(np.uint8))
+        buf = (C.c_uint8 * max(len(blob), 1)).from_buffer_copy(bytes(blob) or b"\0")
+        base = C.addressof(buf)
+        cb = _lib.CCodebook()
+        n, w, s = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        g, b = C.c_void_p(), C.c_void_p()
+        st = L.hgap_container_parse(buf, len(blob), C.byref(cb), C.byref(n), C.byref(w), C.byref(s),
+                                    C.byref(g), C.byref(b))
+        if st != 0:
+            continue
+        accepted += 1
+        assert 1 <= cb.symbol_count <= 256
+        assert s.value == (w.value + 3) // 4
+        gap_bytes = 4 * ((s.value + 7) // 8)
+        assert base <= g.value and g.value + gap_bytes <= base + len(blob)
+        assert base <= b.value and b.value + 4 * w.value <= base + len(blob)
+        lens = [cb.symbols[i].length for i in range(cb.symbol_count)]
+        assert all(1 <= v <= 16 for v in lens) and lens == sorted(lens)
+        assert sum(2.0 ** -v for v in lens) <= 1.0
+    assert accepted > 0  # flips inside the payload leave valid containers
