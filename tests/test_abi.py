@@ -81,6 +81,34 @@ def test_bad_symbol_lists_rejected(syms, lens):
         H.Codebook.from_symbols(syms, lens)
 
 
+def test_symbol_lists_accepted_exactly_when_valid():
+    """Random container-order symbol lists: accepted exactly when the symbols
+    are distinct, the lengths within 1..16 and non-decreasing, and the Kraft
+    sum at most 1; an accepted book's codes are canonical (each code the
+    previous one plus one, shifted to the next length) and prefix-free."""
+    rng = np.random.default_rng(31)
+    for it in range(1500):
+        k = int(rng.integers(1, 40))
+        syms = rng.choice(256, size=k, replace=bool(it % 7 == 0))
+        lens = np.sort(rng.integers(1, 18, size=k)) if it % 5 else rng.integers(1, 17, size=k)
+        valid = (len(set(syms.tolist())) == k and lens.min() >= 1 and lens.max() <= 16
+                 and bool(np.all(np.diff(lens) >= 0)) and sum(2.0 ** -int(v) for v in lens) <= 1.0)
+        if not valid:
+            with pytest.raises(H.HgapError):
+                H.Codebook.from_symbols(syms, lens)
+            continue
+        book = H.Codebook.from_symbols(syms, lens)
+        assert book.symbol_count == k
+        code = prev_len = None
+        for sym, ln in zip(syms.tolist(), lens.tolist()):
+            assert book.length[sym] == ln
+            code = 0 if code is None else (code + 1) << (ln - prev_len)
+            assert book.code[sym] == code
+            prev_len = ln
+        words = sorted(format(int(book.code[v]), f"0{int(book.length[v])}b") for v in syms.tolist())
+        assert all(not b.startswith(a) for a, b in zip(words, words[1:]))
+
+
 def test_container_write_matches_oracle_bytes():
     rng = np.random.default_rng(3)
     r = np.arange(1, 257); p = r ** -1.2; p /= p.sum()
