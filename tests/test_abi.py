@@ -272,3 +272,47 @@ def test_container_parse_survives_random_damage():
         assert all(1 <= v <= 16 for v in lens) and lens == sorted(lens)
         assert sum(2.0 ** -v for v in lens) <= 1.0
     assert accepted > 0  # flips inside the payload leave valid containers
+
+
+def _table_lookup(t1, t2, v):
+    """The decoder's two-level lookup of 16-bit windows v (MSB first): level 1
+    on the top 11 bits; a pointer entry (bit 15: width << 12 | offset) reads
+    level 2 at offset + the next `width` bits.  Returns (symbol, length,
+    invalid) per window."""
+    e = t1[v >> 5].astype(np.int64)
+    ptr = (e & 0x8000) != 0
+    w = (e >> 12) & 7
+    idx = np.where(ptr, (e & 0xFFF) + ((v >> (5 - w)) & ((1 << w) - 1)), 0)
+    e = np.where(ptr, t2[idx].astype(np.int64), e)
+    return e & 0xFF, ((e >> 8) & 15) + 1, (e & 0x4000) != 0
+
+
+def test_host_decode_table_decodes_every_window():
+    """For books from random histograms (complete) and cut-down lists
+    (incomplete), every 16-bit window decodes through the host-built table to
+    the symbol whose code begins it, with that code's length -- and to an
+    invalid entry where no code begins it."""
+    L = _lib.lib()
+    rng = np.random.default_rng(41)
+    v = np.arange(1 << 16, dtype=np.int64)
+    for it in range(120):
+        h = np.zeros(256, np.uint32)
+        k = int(rng.integers(2, 257))
+        h[rng.choice(256, size=k, replace=False)] = (rng.pareto(0.6 + 1.5 * rng.random(), k) * 50 + 1).astype(np.uint32)
+        book, _ = H.Codebook.from_histogram(h)
+        syms, lens = book.symbols, book.lengths
+        if it % 3 == 0 and len(syms) > 2:  # drop codes from the end: an incomplete book
+            cut = int(rng.integers(1, len(syms) - 1))
+            book = H.Codebook.from_symbols(syms[:-cut], lens[:-cut])
+            syms, lens = syms[:-cut], lens[:-cut]
+        t1 = np.zeros(2048, np.uint16)
+        t2 = np.zeros(2560, np.uint16)
+        assert L.hgap_decode_table_build(C.byref(book.cstruct), t1.ctypes.data, t2.ctypes.data) == 0
+        codes = np.array([int(book.code[s]) for s in syms], np.int64)
+        la = codes << (16 - lens.astype(np.int64))  # left-aligned, ascending in container order
+        i = np.searchsorted(la, v, side="right") - 1
+        inside = (i >= 0) & (v - la[np.maximum(i, 0)] < (1 << (16 - lens[np.maximum(i, 0)].astype(np.int64))))
+        sym, ln, bad = _table_lookup(t1, t2, v)
+        assert np.array_equal(bad, ~inside)
+        assert np.array_equal(sym[inside], syms[i[inside]].astype(np.int64))
+        assert np.array_equal(ln[inside], lens[i[inside]].astype(np.int64))
